@@ -1,0 +1,717 @@
+// C-ABI implementation: context, memory, and the plain / learned SpGEMM
+// pipelines.
+//
+// Plain two-pass method (the judge and the fallback):
+//   products -> bin by bound -> symbolic (warp hash / CTA hash / CTA bitmap)
+//   -> bin by exact nnz -> scan -> allocate C -> numeric (warp hash with
+//   per-row sort / column-tiled heavy rows).
+// Learned method:
+//   features + products -> MLP capacity -> bin by capacity -> single numeric
+//   pass into a capacity-sized slab (overflow -> queued) -> exact symbolic for
+//   predicted-heavy and overflowed rows -> scan -> allocate C -> copy slab rows
+//   + numeric pass for the exact rows.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "context.hpp"
+
+using namespace spg;
+
+namespace spg {
+
+spg_status fail(spg_ctx* ctx, spg_status st, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->last_error = buf;
+  }
+  return st;
+}
+
+spg_status cuda_status(spg_ctx* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return SPG_OK;
+  const spg_status st = (e == cudaErrorMemoryAllocation) ? SPG_ERR_OUT_OF_MEMORY : SPG_ERR_CUDA;
+  (void)cudaGetLastError();  // clear a sticky-free error so the context stays usable
+  return fail(ctx, st, "%s: %s", what, cudaGetErrorString(e));
+}
+
+spg_status DevBuf::alloc(spg_ctx* ctx, size_t bytes) {
+  reset();
+  ctx_ = ctx;
+  if (bytes == 0) return SPG_OK;
+  cudaError_t e = cudaMallocAsync(&ptr_, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    ptr_ = nullptr;
+    return cuda_status(ctx, e, "cudaMallocAsync");
+  }
+  return SPG_OK;
+}
+
+void DevBuf::reset() {
+  if (ptr_ && ctx_) cudaFreeAsync(ptr_, ctx_->stream);
+  ptr_ = nullptr;
+}
+
+spg_tuning default_tuning() {
+  spg_tuning t{};
+  t.warp_table_max = 4096;
+  t.warps_per_block = 8;
+  t.max_load = 0.5f;
+  t.tile_cols = kTileCols;
+  t.block_table_max = 16384;
+  t.predict_margin = 1.25f;
+  t.predict_slack = 8;
+  return t;
+}
+
+static int ilog2_floor(int64_t v) {
+  int l = 0;
+  while ((int64_t(1) << (l + 1)) <= v) ++l;
+  return l;
+}
+
+BinParams bin_params(const spg_tuning& t) {
+  BinParams bp{};
+  int lg = ilog2_floor(std::max(32, std::min(4096, t.warp_table_max)));
+  bp.warp_log_max = std::max(kMinLogT, std::min(kMaxLogT, lg));
+  bp.max_load = std::min(0.9f, std::max(0.1f, t.max_load));
+  bp.warp_cap = (int64_t)std::floor((double)(1 << bp.warp_log_max) * bp.max_load);
+  // symbolic CTA table at load <= 2/3
+  int blg = ilog2_floor(std::max(1024, std::min(32768, t.block_table_max)));
+  bp.block_cap = ((int64_t)1 << blg) * 2 / 3;
+  return bp;
+}
+
+static int block_table_log(const spg_tuning& t) {
+  return ilog2_floor(std::max(1024, std::min(32768, t.block_table_max)));
+}
+
+spg_status read_flags(spg_ctx* ctx, int* flags) {
+  SPG_CUDA(ctx, cudaMemcpyAsync(&ctx->h_stage[15], ctx->d_flags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  int f = 0;
+  std::memcpy(&f, &ctx->h_stage[15], sizeof(int));
+  if (f) SPG_CUDA(ctx, cudaMemsetAsync(ctx->d_flags, 0, sizeof(int), ctx->stream));
+  *flags = f;
+  return SPG_OK;
+}
+
+spg_status prepare_matrix(spg_ctx* ctx, const spg_csr* m, DevMat& out, bool validate) {
+  if (!m) return fail(ctx, SPG_ERR_INVALID_ARG, "null matrix");
+  if (m->rows < 0 || m->cols < 0 || m->nnz < 0) return fail(ctx, SPG_ERR_INVALID_ARG, "negative dimension");
+  if (m->cols > INT32_MAX) return fail(ctx, SPG_ERR_UNSUPPORTED, "more than 2^31-1 columns");
+  if (m->index_bits != 32 && m->index_bits != 64) return fail(ctx, SPG_ERR_INVALID_ARG, "index_bits must be 32 or 64");
+  if (m->rows > 0 && !m->row_ptr) return fail(ctx, SPG_ERR_INVALID_ARG, "null row_ptr");
+  if (m->nnz > 0 && (!m->col_idx || !m->val)) return fail(ctx, SPG_ERR_INVALID_ARG, "null col_idx/val");
+  if (m->index_bits == 32 && m->nnz > INT32_MAX) return fail(ctx, SPG_ERR_INVALID_ARG, "nnz overflows int32 row_ptr");
+  const LaunchCtx lc = launch_ctx(ctx);
+  const size_t rp_bytes = (size_t)(m->rows + 1) * (m->index_bits / 8);
+  const void* rp = m->row_ptr;
+  const int32_t* col = m->col_idx;
+  const float* val = m->val;
+  if (m->location == SPG_HOST) {
+    SPG_TRY(out.upload[0].alloc(ctx, rp_bytes));
+    SPG_TRY(out.upload[1].alloc(ctx, (size_t)m->nnz * 4));
+    SPG_TRY(out.upload[2].alloc(ctx, (size_t)m->nnz * 4));
+    if (m->rows >= 0)
+      SPG_CUDA(ctx, cudaMemcpyAsync(out.upload[0].get(), m->row_ptr, rp_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    if (m->nnz > 0) {
+      SPG_CUDA(ctx, cudaMemcpyAsync(out.upload[1].get(), m->col_idx, (size_t)m->nnz * 4, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+      SPG_CUDA(ctx, cudaMemcpyAsync(out.upload[2].get(), m->val, (size_t)m->nnz * 4, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+    }
+    rp = out.upload[0].get();
+    col = out.upload[1].as<int32_t>();
+    val = out.upload[2].as<float>();
+  } else if (m->location != SPG_DEVICE) {
+    return fail(ctx, SPG_ERR_INVALID_ARG, "location must be SPG_HOST or SPG_DEVICE");
+  }
+  const int64_t* rp64;
+  if (m->index_bits == 32) {
+    SPG_TRY(out.rp64.alloc(ctx, (size_t)(m->rows + 1) * 8));
+    launch_widen_rp(static_cast<const int32_t*>(rp), m->rows + 1, out.rp64.as<int64_t>(), lc);
+    ++ctx->launches;
+    rp64 = out.rp64.as<int64_t>();
+  } else {
+    rp64 = static_cast<const int64_t*>(rp);
+  }
+  out.view = DCsr{m->rows, m->cols, rp64, col, val};
+  out.nnz = m->nnz;
+  if (validate) {
+    launch_validate(out.view, m->nnz, ctx->d_flags, lc);
+    ++ctx->launches;
+  }
+  return SPG_OK;
+}
+
+StageTimer::StageTimer(spg_ctx* ctx, bool enabled) : ctx_(ctx), on_(enabled) {
+  cudaEventCreate(&start_);
+  cudaEventCreate(&end_);
+  cudaEventRecord(start_, ctx->stream);
+}
+
+StageTimer::~StageTimer() {
+  for (auto& m : marks_) cudaEventDestroy(m.second);
+  cudaEventDestroy(start_);
+  cudaEventDestroy(end_);
+}
+
+void StageTimer::mark(int stage) {
+  if (!on_) return;
+  cudaEvent_t ev;
+  cudaEventCreate(&ev);
+  cudaEventRecord(ev, ctx_->stream);
+  marks_.emplace_back(stage, ev);
+}
+
+void StageTimer::finish(spg_report* rep) {
+  cudaEventRecord(end_, ctx_->stream);
+  cudaEventSynchronize(end_);
+  if (!rep) return;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, start_, end_);
+  rep->ms_total = ms;
+  for (size_t i = 0; i < marks_.size(); ++i) {
+    cudaEvent_t next = (i + 1 < marks_.size()) ? marks_[i + 1].second : end_;
+    float d = 0.f;
+    cudaEventElapsedTime(&d, marks_[i].second, next);
+    const int st = marks_[i].first;
+    if (st >= 0 && st < SPG_STAGE_COUNT) rep->ms_stage[st] += d;
+  }
+}
+
+}  // namespace spg
+
+// ===========================================================================
+// Pipelines
+// ===========================================================================
+
+namespace {
+
+// Buffers and host mirrors of one multiply call.
+struct Pipeline {
+  spg_ctx* ctx;
+  LaunchCtx lc;
+  const DevMat& A;
+  const DevMat& B;
+  spg_tuning tune;
+  BinParams bp;
+  int64_t rows, cols;
+  int ntiles;
+  int wpb;
+
+  DevBuf prod;        // int64 rows
+  DevBuf nnz;         // int64 rows+1 (becomes C's row pointers)
+  DevBuf bin_of_row;  // uint8 rows
+  DevBuf binmeta;     // int64: counts[12] offsets[13] cursors[12]
+  DevBuf lists;       // int32 rows
+  DevBuf big_slot;    // int32 rows
+  DevBuf tile_cnt;    // int32 nbig * ntiles
+  DevBuf tile_off;    // int32 nbig * ntiles
+  DevBuf scan_tmp;    // int64
+  int64_t h_off[kNumBins + 1] = {};
+  int64_t nbig = 0;
+
+  Pipeline(spg_ctx* c, const DevMat& a, const DevMat& b, const spg_tuning& t)
+      : ctx(c), lc(launch_ctx(c)), A(a), B(b), tune(t), bp(bin_params(t)), rows(a.view.rows), cols(b.view.cols) {
+    ntiles = (int)std::max<int64_t>(1, (cols + kTileCols - 1) / kTileCols);
+    wpb = std::max(1, std::min(16, t.warps_per_block));
+  }
+
+  int64_t* counts() { return binmeta.as<int64_t>(); }
+  int64_t* offsets() { return binmeta.as<int64_t>() + kNumBins; }
+  int64_t* cursors() { return binmeta.as<int64_t>() + 2 * kNumBins + 1; }
+
+  spg_status init() {
+    SPG_TRY(prod.alloc(ctx, (size_t)std::max<int64_t>(rows, 1) * 8));
+    SPG_TRY(nnz.alloc(ctx, (size_t)(rows + 1) * 8));
+    SPG_TRY(bin_of_row.alloc(ctx, (size_t)std::max<int64_t>(rows, 1)));
+    SPG_TRY(binmeta.alloc(ctx, (size_t)(3 * kNumBins + 1) * 8));
+    SPG_TRY(lists.alloc(ctx, (size_t)std::max<int64_t>(rows, 1) * 4));
+    SPG_TRY(big_slot.alloc(ctx, (size_t)std::max<int64_t>(rows, 1) * 4));
+    SPG_TRY(scan_tmp.alloc(ctx, (size_t)scan_temp_elems(rows + 1) * 8));
+    SPG_CUDA(ctx, cudaMemsetAsync(nnz.get(), 0, (size_t)(rows + 1) * 8, ctx->stream));
+    return SPG_OK;
+  }
+
+  void bin(const int64_t* key, int mode) {
+    launch_binning(key, rows, cols, mode, bp, bin_of_row.as<uint8_t>(), counts(), offsets(), cursors(),
+                   lists.as<int32_t>(), lc);
+    ctx->launches += 3;
+  }
+
+  // Offsets of the last binning (and optional extra int64 words) to host.
+  spg_status fetch_offsets(const int64_t* extra = nullptr, int64_t* extra_host = nullptr, int n_extra = 0) {
+    SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage, offsets(), sizeof(int64_t) * (kNumBins + 1), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    for (int i = 0; i < n_extra; ++i)
+      SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kNumBins + 1 + i, extra + i, sizeof(int64_t),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+    SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::memcpy(h_off, ctx->h_stage, sizeof(int64_t) * (kNumBins + 1));
+    for (int i = 0; i < n_extra; ++i) extra_host[i] = ctx->h_stage[kNumBins + 1 + i];
+    return SPG_OK;
+  }
+
+  int64_t bin_size(int b) const { return h_off[b + 1] - h_off[b]; }
+  const int32_t* bin_rows(int b) { return lists.as<int32_t>() + h_off[b]; }
+
+  // Exact symbolic pass over rows whose key (products) is > 0.
+  spg_status symbolic(const int64_t* key) {
+    bin(key, kBinSymbolic);
+    SPG_TRY(fetch_offsets());
+    for (int b = 0; b < kNumWarpBins; ++b) {
+      if (bin_size(b) == 0) continue;
+      launch_sym_warp(kMinLogT + b, A.view, B.view, bin_rows(b), bin_size(b), nnz.as<int64_t>(), ctx->d_flags, lc,
+                      wpb);
+      ++ctx->launches;
+    }
+    const int64_t nblock = bin_size(kBinBlock), ndense = bin_size(kBinDense);
+    nbig = nblock + ndense;
+    if (nbig > 0) {
+      const size_t tb = (size_t)nbig * ntiles * 4;
+      SPG_TRY(tile_cnt.alloc(ctx, tb));
+      SPG_TRY(tile_off.alloc(ctx, tb));
+      SPG_CUDA(ctx, cudaMemsetAsync(tile_cnt.get(), 0, tb, ctx->stream));
+      if (nblock) {
+        launch_sym_block(A.view, B.view, bin_rows(kBinBlock), nblock, block_table_log(tune), 0, nnz.as<int64_t>(),
+                         big_slot.as<int32_t>(), tile_cnt.as<int32_t>(), ntiles, ctx->d_flags, lc);
+        ++ctx->launches;
+      }
+      if (ndense) {
+        launch_sym_dense(A.view, B.view, bin_rows(kBinDense), ndense, nblock, nnz.as<int64_t>(),
+                         big_slot.as<int32_t>(), tile_cnt.as<int32_t>(), ntiles, ctx->d_flags, lc);
+        ++ctx->launches;
+      }
+    }
+    return SPG_OK;
+  }
+
+  // Numeric pass for the rows in the current (numeric) binning, into C.
+  spg_status numeric(const int64_t* c_rp, int32_t* c_col, float* c_val, spg_report* rep) {
+    for (int b = 0; b < kNumWarpBins; ++b) {
+      if (bin_size(b) == 0) continue;
+      launch_num_warp(kMinLogT + b, A.view, B.view, bin_rows(b), bin_size(b), c_rp, c_col, c_val, ctx->d_flags, lc,
+                      wpb);
+      ++ctx->launches;
+    }
+    const int64_t nheavy = bin_size(kBinHeavy);
+    if (nheavy > 0) {
+      launch_tile_offsets(bin_rows(kBinHeavy), nheavy, big_slot.as<int32_t>(), tile_cnt.as<int32_t>(), ntiles,
+                          tile_off.as<int32_t>(), lc);
+      launch_num_tile(A.view, B.view, bin_rows(kBinHeavy), nheavy, big_slot.as<int32_t>(), tile_cnt.as<int32_t>(),
+                      tile_off.as<int32_t>(), ntiles, c_rp, c_col, c_val, ctx->d_counter, ctx->d_flags, lc);
+      ctx->launches += 3;
+    }
+    if (rep) {
+      for (int b = 0; b < kNumBins && b < SPG_NUM_BINS; ++b) rep->bin_rows[b] += bin_size(b);
+      rep->rows_heavy += nheavy;
+    }
+    return SPG_OK;
+  }
+};
+
+// Fills C from the pipeline's row pointers and the col/val buffers; narrows
+// the row pointers to int32 when requested or when nnz(C) fits.
+spg_status finish_output(spg_ctx* ctx, Pipeline& P, int64_t total, const spg_opts& o, DevBuf& c_col, DevBuf& c_val,
+                         spg_csr* C) {
+  int bits = o.out_index_bits;
+  if (bits == 0) bits = total < INT32_MAX ? 32 : 64;
+  if (bits != 32 && bits != 64) return fail(ctx, SPG_ERR_INVALID_ARG, "out_index_bits must be 0, 32 or 64");
+  if (bits == 32 && total >= INT32_MAX)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "nnz(C)=%lld does not fit int32 row pointers", (long long)total);
+  const LaunchCtx lc = launch_ctx(ctx);
+  void* rp = nullptr;
+  if (bits == 64) {
+    rp = P.nnz.release();
+  } else {
+    DevBuf rp32;
+    SPG_TRY(rp32.alloc(ctx, (size_t)(P.rows + 1) * 4));
+    launch_narrow_rp(P.nnz.as<int64_t>(), P.rows + 1, rp32.as<int32_t>(), lc);
+    ++ctx->launches;
+    rp = rp32.release();
+  }
+  std::memset(C, 0, sizeof *C);
+  C->rows = P.rows;
+  C->cols = P.cols;
+  C->nnz = total;
+  C->capacity = total;
+  C->index_bits = bits;
+  C->location = SPG_DEVICE;
+  C->row_ptr = rp;
+  C->col_idx = static_cast<int32_t*>(c_col.release());
+  C->val = static_cast<float*>(c_val.release());
+  C->owner = 1;
+  return SPG_OK;
+}
+
+spg_status check_flags(spg_ctx* ctx, spg_report* rep) {
+  int f = 0;
+  SPG_TRY(read_flags(ctx, &f));
+  if (rep) rep->device_flags |= f;
+  if (f & kFlagBadIndex) return fail(ctx, SPG_ERR_INVALID_ARG, "input failed validation (index out of range, "
+                                                               "unsorted or duplicate columns, bad row pointers)");
+  if (f & (kFlagHashFull | kFlagCountDiff)) return fail(ctx, SPG_ERR_INTERNAL, "device consistency check failed (flags %d)", f);
+  if (f & kFlagWaitLimit) return fail(ctx, SPG_ERR_TIMEOUT, "a bounded device wait gave up");
+  return SPG_OK;
+}
+
+spg_status multiply_plain(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opts& o, spg_report* rep,
+                          StageTimer& tm) {
+  const LaunchCtx lc = P.lc;
+  tm.mark(SPG_STAGE_PRODUCTS);
+  launch_row_products(P.A.view, P.B.view, P.prod.as<int64_t>(), lc);
+  SPG_CUDA(ctx, cudaMemsetAsync(ctx->d_counter + 1, 0, 8, ctx->stream));
+  launch_sum(P.prod.as<int64_t>(), P.rows, ctx->d_counter + 1, lc);
+  ctx->launches += 2;
+  tm.mark(SPG_STAGE_SYMBOLIC);
+  SPG_TRY(P.symbolic(P.prod.as<int64_t>()));
+  tm.mark(SPG_STAGE_BINNING);
+  P.bin(P.nnz.as<int64_t>(), kBinNumeric);
+  tm.mark(SPG_STAGE_SCAN);
+  launch_excl_scan(P.nnz.as<int64_t>(), P.rows, P.nnz.as<int64_t>(), P.scan_tmp.as<int64_t>(), lc);
+  ctx->launches += 4;
+  int64_t extra[2];
+  const int64_t* src[2] = {P.nnz.as<int64_t>() + P.rows, reinterpret_cast<const int64_t*>(ctx->d_counter + 1)};
+  // fetch offsets + total nnz + products
+  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage, P.offsets(), sizeof(int64_t) * (kNumBins + 1), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kNumBins + 1, src[0], 8, cudaMemcpyDeviceToHost, ctx->stream));
+  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kNumBins + 2, src[1], 8, cudaMemcpyDeviceToHost, ctx->stream));
+  SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memcpy(P.h_off, ctx->h_stage, sizeof(int64_t) * (kNumBins + 1));
+  extra[0] = ctx->h_stage[kNumBins + 1];
+  extra[1] = ctx->h_stage[kNumBins + 2];
+  const int64_t total = extra[0];
+  if (rep) rep->products = extra[1];
+  DevBuf c_col, c_val;
+  SPG_TRY(c_col.alloc(ctx, (size_t)total * 4));
+  SPG_TRY(c_val.alloc(ctx, (size_t)total * 4));
+  tm.mark(SPG_STAGE_NUMERIC);
+  SPG_TRY(P.numeric(P.nnz.as<int64_t>(), c_col.as<int32_t>(), c_val.as<float>(), rep));
+  SPG_TRY(finish_output(ctx, P, total, o, c_col, c_val, C));
+  if (rep) rep->nnz_c = total;
+  return SPG_OK;
+}
+
+spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opts& o, spg_report* rep,
+                            StageTimer& tm) {
+  const LaunchCtx lc = P.lc;
+  SPG_TRY(ensure_mlp(ctx));
+  const int64_t rows = P.rows;
+  DevBuf feats, cap, need, slab_off, key;
+  SPG_TRY(feats.alloc(ctx, (size_t)std::max<int64_t>(rows, 1) * kMlpIn * 4));
+  SPG_TRY(cap.alloc(ctx, (size_t)(rows + 1) * 8));
+  SPG_TRY(need.alloc(ctx, (size_t)std::max<int64_t>(rows, 1)));
+  SPG_TRY(slab_off.alloc(ctx, (size_t)(rows + 1) * 8));
+  SPG_TRY(key.alloc(ctx, (size_t)std::max<int64_t>(rows, 1) * 8));
+  tm.mark(SPG_STAGE_FEATURES);
+  launch_features(P.A.view, P.B.view, feats.as<float>(), P.prod.as<int64_t>(), lc);
+  SPG_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, 4 * 8, ctx->stream));
+  launch_sum(P.prod.as<int64_t>(), rows, ctx->d_counter + 1, lc);
+  tm.mark(SPG_STAGE_MLP);
+  launch_mlp_capacity(ctx->mlp_w16, feats.as<float>(), P.prod.as<int64_t>(), rows, P.cols, P.tune.predict_margin,
+                      P.tune.predict_slack, P.bp.warp_cap, o.force_overflow, cap.as<int64_t>(), need.as<uint8_t>(),
+                      lc);
+  ctx->launches += 3;
+  tm.mark(SPG_STAGE_BINNING);
+  P.bin(cap.as<int64_t>(), kBinLearned);
+  launch_excl_scan(cap.as<int64_t>(), rows, slab_off.as<int64_t>(), P.scan_tmp.as<int64_t>(), lc);
+  ctx->launches += 4;
+  int64_t slab_total = 0;
+  SPG_TRY(P.fetch_offsets(slab_off.as<int64_t>() + rows, &slab_total, 1));
+  int64_t light = 0;
+  for (int b = 0; b < kNumWarpBins; ++b) light += P.bin_size(b);
+  if (rep) rep->rows_predicted = light;
+  // single numeric pass for the predicted-light rows
+  DevBuf slab_col, slab_val, retry;
+  SPG_TRY(slab_col.alloc(ctx, (size_t)slab_total * 4));
+  SPG_TRY(slab_val.alloc(ctx, (size_t)slab_total * 4));
+  SPG_TRY(retry.alloc(ctx, (size_t)std::max<int64_t>(light, 1) * 4));
+  tm.mark(SPG_STAGE_NUMERIC);
+  for (int b = 0; b < kNumWarpBins; ++b) {
+    if (P.bin_size(b) == 0) continue;
+    launch_num_warp_learned(kMinLogT + b, P.A.view, P.B.view, P.bin_rows(b), P.bin_size(b), cap.as<int64_t>(),
+                            slab_off.as<int64_t>(), slab_col.as<int32_t>(), slab_val.as<float>(), P.nnz.as<int64_t>(),
+                            retry.as<int32_t>(), ctx->d_counter + 2, ctx->d_flags, lc, P.wpb);
+    ++ctx->launches;
+  }
+  // keep the light-row list for the compaction copy
+  DevBuf light_rows;
+  SPG_TRY(light_rows.alloc(ctx, (size_t)std::max<int64_t>(light, 1) * 4));
+  if (light)
+    SPG_CUDA(ctx, cudaMemcpyAsync(light_rows.get(), P.lists.get(), (size_t)light * 4, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+  // exact path: predicted-heavy rows plus overflowed rows
+  tm.mark(SPG_STAGE_FIXUP);
+  launch_mark_rows(retry.as<int32_t>(), ctx->d_counter + 2, need.as<uint8_t>(), lc);
+  launch_mask_key(P.prod.as<int64_t>(), need.as<uint8_t>(), rows, key.as<int64_t>(), lc);
+  ctx->launches += 2;
+  SPG_TRY(P.symbolic(key.as<int64_t>()));
+  launch_mask_key(P.nnz.as<int64_t>(), need.as<uint8_t>(), rows, key.as<int64_t>(), lc);
+  P.bin(key.as<int64_t>(), kBinNumeric);
+  ctx->launches += 1;
+  tm.mark(SPG_STAGE_SCAN);
+  launch_excl_scan(P.nnz.as<int64_t>(), rows, P.nnz.as<int64_t>(), P.scan_tmp.as<int64_t>(), lc);
+  ctx->launches += 4;
+  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage, P.offsets(), sizeof(int64_t) * (kNumBins + 1), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kNumBins + 1, P.nnz.as<int64_t>() + rows, 8, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kNumBins + 2, ctx->d_counter + 1, 16, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memcpy(P.h_off, ctx->h_stage, sizeof(int64_t) * (kNumBins + 1));
+  const int64_t total = ctx->h_stage[kNumBins + 1];
+  if (rep) {
+    rep->products = ctx->h_stage[kNumBins + 2];
+    rep->rows_overflow = ctx->h_stage[kNumBins + 3];
+  }
+  DevBuf c_col, c_val;
+  SPG_TRY(c_col.alloc(ctx, (size_t)total * 4));
+  SPG_TRY(c_val.alloc(ctx, (size_t)total * 4));
+  tm.mark(SPG_STAGE_COMPACT);
+  launch_compact_rows(light_rows.as<int32_t>(), light, need.as<uint8_t>(), slab_off.as<int64_t>(),
+                      slab_col.as<int32_t>(), slab_val.as<float>(), P.nnz.as<int64_t>(), c_col.as<int32_t>(),
+                      c_val.as<float>(), lc);
+  ++ctx->launches;
+  tm.mark(SPG_STAGE_NUMERIC);
+  SPG_TRY(P.numeric(P.nnz.as<int64_t>(), c_col.as<int32_t>(), c_val.as<float>(), rep));
+  SPG_TRY(finish_output(ctx, P, total, o, c_col, c_val, C));
+  if (rep) rep->nnz_c = total;
+  return SPG_OK;
+}
+
+}  // namespace
+
+namespace spg {
+
+spg_status multiply_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, spg_csr* C, const spg_opts& o,
+                           spg_report* rep) {
+  StageTimer tm(ctx, o.stage_timing != 0);
+  const spg_tuning t = o.use_tuning ? ctx->tuning : default_tuning();
+  Pipeline P(ctx, A, B, t);
+  SPG_TRY(P.init());
+  spg_status st = (o.algo == SPG_ALGO_LEARNED) ? multiply_learned(ctx, P, C, o, rep, tm)
+                                               : multiply_plain(ctx, P, C, o, rep, tm);
+  if (st != SPG_OK) return st;
+  tm.finish(rep);
+  return check_flags(ctx, rep);
+}
+
+spg_status row_nnz_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, int64_t* d_nnz) {
+  Pipeline P(ctx, A, B, ctx->tuning);
+  SPG_TRY(P.init());
+  launch_row_products(A.view, B.view, P.prod.as<int64_t>(), P.lc);
+  SPG_TRY(P.symbolic(P.prod.as<int64_t>()));
+  if (P.rows)
+    SPG_CUDA(ctx, cudaMemcpyAsync(d_nnz, P.nnz.get(), (size_t)P.rows * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  return check_flags(ctx, nullptr);
+}
+
+}  // namespace spg
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+int32_t spg_version(void) { return 10000; }
+
+const char* spg_status_string(spg_status s) {
+  switch (s) {
+    case SPG_OK: return "ok";
+    case SPG_ERR_INVALID_ARG: return "invalid argument";
+    case SPG_ERR_CUDA: return "CUDA error";
+    case SPG_ERR_OUT_OF_MEMORY: return "out of memory";
+    case SPG_ERR_IO: return "I/O error";
+    case SPG_ERR_FORMAT: return "malformed Matrix Market file";
+    case SPG_ERR_TIMEOUT: return "device wait timed out";
+    case SPG_ERR_UNSUPPORTED: return "unsupported";
+    case SPG_ERR_INTERNAL: return "internal consistency check failed";
+    default: return "unknown status";
+  }
+}
+
+spg_status spg_create(spg_ctx** out, int32_t device) {
+  if (!out) return SPG_ERR_INVALID_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    (void)cudaGetLastError();
+    return SPG_ERR_CUDA;
+  }
+  if (device < 0 || device >= n) return SPG_ERR_INVALID_ARG;
+  std::unique_ptr<spg_ctx> ctx(new (std::nothrow) spg_ctx());
+  if (!ctx) return SPG_ERR_OUT_OF_MEMORY;
+  ctx->device = device;
+  SPG_CUDA(ctx.get(), cudaSetDevice(device));
+  cudaDeviceProp prop{};
+  SPG_CUDA(ctx.get(), cudaGetDeviceProperties(&prop, device));
+  ctx->sms = prop.multiProcessorCount;
+  ctx->gpu_name = prop.name;
+  SPG_CUDA(ctx.get(), cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+  ctx->stream = ctx->own_stream;
+  SPG_CUDA(ctx.get(), cudaDeviceGetDefaultMemPool(&ctx->pool, device));
+  uint64_t thr = UINT64_MAX;
+  SPG_CUDA(ctx.get(), cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  SPG_CUDA(ctx.get(), cudaMalloc(&ctx->d_flags, 64));
+  SPG_CUDA(ctx.get(), cudaMemset(ctx->d_flags, 0, 64));
+  SPG_CUDA(ctx.get(), cudaMalloc(&ctx->d_counter, 8 * sizeof(unsigned long long)));
+  SPG_CUDA(ctx.get(), cudaMemset(ctx->d_counter, 0, 8 * sizeof(unsigned long long)));
+  SPG_CUDA(ctx.get(), cudaMallocHost(&ctx->h_stage, 64 * sizeof(int64_t)));
+  ctx->tuning = default_tuning();
+  *out = ctx.release();
+  return SPG_OK;
+}
+
+spg_status spg_destroy(spg_ctx* ctx) {
+  if (!ctx) return SPG_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  spg::free_batch_cache(ctx);
+  cudaFree(ctx->mlp_master);
+  cudaFree(ctx->mlp_w16);
+  cudaFree(ctx->d_flags);
+  cudaFree(ctx->d_counter);
+  cudaFreeHost(ctx->h_stage);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return SPG_OK;
+}
+
+const char* spg_last_error(const spg_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+spg_status spg_set_stream(spg_ctx* ctx, void* stream) {
+  if (!ctx) return SPG_ERR_INVALID_ARG;
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return SPG_OK;
+}
+
+void* spg_get_stream(const spg_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+spg_status spg_multiply(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_csr* C, const spg_opts* opts,
+                        spg_report* report) {
+  if (!ctx) return SPG_ERR_INVALID_ARG;
+  if (!A || !B || !C) return fail(ctx, SPG_ERR_INVALID_ARG, "null argument");
+  if (A->cols != B->rows)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "inner dimensions differ (%lld vs %lld)", (long long)A->cols,
+                (long long)B->rows);
+  if (A->rows > INT32_MAX) return fail(ctx, SPG_ERR_UNSUPPORTED, "more than 2^31-1 rows");
+  SPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  spg_opts o{};
+  if (opts) o = *opts;
+  if (report) {
+    std::memset(report, 0, sizeof *report);
+    report->algo = o.algo;
+    report->rows = A->rows;
+  }
+  const int launches0 = ctx->launches;
+  StageTimer outer(ctx, false);
+  DevMat dA, dB;
+  SPG_TRY(prepare_matrix(ctx, A, dA, !o.skip_validation));
+  SPG_TRY(prepare_matrix(ctx, B, dB, !o.skip_validation));
+  if (!o.skip_validation) SPG_TRY(check_flags(ctx, report));
+  spg_csr dev_c{};
+  spg_status st;
+  if (o.algo == SPG_ALGO_CUSPARSE) st = multiply_cusparse(ctx, dA, dB, &dev_c, o, report);
+  else if (o.algo == SPG_ALGO_PLAIN || o.algo == SPG_ALGO_LEARNED) st = multiply_device(ctx, dA, dB, &dev_c, o, report);
+  else return fail(ctx, SPG_ERR_INVALID_ARG, "unknown algo %d", o.algo);
+  if (st != SPG_OK) {
+    spg_csr_free(ctx, &dev_c);
+    return st;
+  }
+  if (o.out_location == SPG_HOST) {
+    spg_csr host_c{};
+    st = spg_csr_copy(ctx, &dev_c, SPG_HOST, &host_c);
+    spg_csr_free(ctx, &dev_c);
+    if (st != SPG_OK) return st;
+    *C = host_c;
+  } else {
+    *C = dev_c;
+  }
+  if (report) {
+    outer.finish(nullptr);
+    report->kernel_launches = ctx->launches - launches0;
+    // whole-call device time, including uploads and the host copy
+    float ms = 0.f;
+    (void)ms;
+  }
+  return SPG_OK;
+}
+
+spg_status spg_csr_free(spg_ctx* ctx, spg_csr* m) {
+  if (!m || m->owner == 0) return SPG_OK;
+  if (m->owner == 1) {
+    cudaStream_t s = ctx ? ctx->stream : nullptr;
+    if (m->row_ptr) cudaFreeAsync(m->row_ptr, s);
+    if (m->col_idx) cudaFreeAsync(m->col_idx, s);
+    if (m->val) cudaFreeAsync(m->val, s);
+  } else if (m->owner == 2) {
+    free(m->row_ptr);
+    free(m->col_idx);
+    free(m->val);
+  } else if (m->owner == 3) {
+    cudaFreeHost(m->row_ptr);
+    cudaFreeHost(m->col_idx);
+    cudaFreeHost(m->val);
+  }
+  m->row_ptr = nullptr;
+  m->col_idx = nullptr;
+  m->val = nullptr;
+  m->owner = 0;
+  return SPG_OK;
+}
+
+spg_status spg_csr_copy(spg_ctx* ctx, const spg_csr* src, int32_t location, spg_csr* dst) {
+  if (!ctx || !src || !dst) return SPG_ERR_INVALID_ARG;
+  if (location != SPG_HOST && location != SPG_DEVICE) return fail(ctx, SPG_ERR_INVALID_ARG, "bad location");
+  spg_csr d = *src;
+  d.location = location;
+  d.capacity = src->nnz;
+  const size_t rpb = (size_t)(src->rows + 1) * (src->index_bits / 8);
+  const size_t nb = (size_t)src->nnz * 4;
+  const cudaMemcpyKind kind =
+      src->location == SPG_HOST ? (location == SPG_HOST ? cudaMemcpyHostToHost : cudaMemcpyHostToDevice)
+                                : (location == SPG_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice);
+  if (location == SPG_HOST) {
+    d.owner = 2;
+    d.row_ptr = malloc(std::max<size_t>(rpb, 1));
+    d.col_idx = (int32_t*)malloc(std::max<size_t>(nb, 1));
+    d.val = (float*)malloc(std::max<size_t>(nb, 1));
+    if (!d.row_ptr || !d.col_idx || !d.val) {
+      free(d.row_ptr);
+      free(d.col_idx);
+      free(d.val);
+      return fail(ctx, SPG_ERR_OUT_OF_MEMORY, "host allocation of %zu bytes failed", rpb + 2 * nb);
+    }
+  } else {
+    d.owner = 1;
+    DevBuf a, b, c;
+    SPG_TRY(a.alloc(ctx, std::max<size_t>(rpb, 4)));
+    SPG_TRY(b.alloc(ctx, std::max<size_t>(nb, 4)));
+    SPG_TRY(c.alloc(ctx, std::max<size_t>(nb, 4)));
+    d.row_ptr = a.release();
+    d.col_idx = (int32_t*)b.release();
+    d.val = (float*)c.release();
+  }
+  if (rpb) SPG_CUDA(ctx, cudaMemcpyAsync(d.row_ptr, src->row_ptr, rpb, kind, ctx->stream));
+  if (nb) {
+    SPG_CUDA(ctx, cudaMemcpyAsync(d.col_idx, src->col_idx, nb, kind, ctx->stream));
+    SPG_CUDA(ctx, cudaMemcpyAsync(d.val, src->val, nb, kind, ctx->stream));
+  }
+  SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *dst = d;
+  return SPG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,198 @@
+// Device-side building blocks shared by every SpGEMM kernel of the engine.
+//
+// Arithmetic contract (restated from the reference's any-hit accumulate,
+// optixSpMSpM/src/optixSpMSpM/optixSpMSpM.cu:246-258): each intermediate
+// product is rounded to FP32 (__fmul_rn) and then added in FP32 (__fadd_rn);
+// no fused multiply-add.  Every accumulator adds the products of one output
+// entry in canonical order: k ascending through A's row, then j ascending
+// through B's row k.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace spg {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int32_t kEmpty = -1;        // empty hash-table key
+constexpr int kTileShift = 13;        // heavy-row column tile: 8192 columns
+constexpr int kTileCols = 1 << kTileShift;
+constexpr int kTileWords = kTileCols / 32;
+
+// Device error flags (mirrors SPG_FLAG_* of the public header).
+constexpr int kFlagHashFull = 1;
+constexpr int kFlagWaitLimit = 2;
+constexpr int kFlagBadIndex = 4;
+constexpr int kFlagCountDiff = 8;
+
+// Read-only device view of a CSR matrix with 64-bit row pointers.
+struct DCsr {
+  int64_t rows;
+  int64_t cols;
+  const int64_t* rp;
+  const int32_t* col;
+  const float* val;
+};
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+__device__ __forceinline__ void raise_flag(int* flags, int f) {
+  if (flags) atomicOr(flags, f);
+}
+
+// Multiplicative (Fibonacci) hash of a column index into 2^log_t slots.
+__device__ __forceinline__ uint32_t hash_slot(int32_t j, int log_t) {
+  return ((uint32_t)j * 2654435761u) >> (32 - log_t);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    T w = __shfl_xor_sync(kFull, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    T w = __shfl_xor_sync(kFull, v, o);
+    v = w < v ? w : v;
+  }
+  return v;
+}
+
+// Inclusive prefix sum across the warp.
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T w = __shfl_up_sync(kFull, v, o);
+    if (lane >= o) v += w;
+  }
+  return v;
+}
+
+// First lane l whose (nondecreasing) inclusive prefix incl[l] exceeds t.
+// Requires t < incl[31].
+__device__ __forceinline__ int warp_upper_bound(int incl, int t) {
+  int lo = 0;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    int v = __shfl_sync(kFull, incl, lo + s - 1);
+    if (v <= t) lo += s;
+  }
+  return lo;
+}
+
+// Product in the reference's arithmetic: rounded to FP32, no contraction.
+__device__ __forceinline__ float prod_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+// Inserts key j into an open-addressing table of 2^log_t slots (linear
+// probing).  Returns the slot and sets `fresh` when the key was new.
+// Gives up after 2^log_t probes (table full): returns -1 and raises a flag.
+__device__ __forceinline__ int hash_insert(int32_t* keys, int log_t, int32_t j, bool& fresh,
+                                           int* flags) {
+  const uint32_t mask = (1u << log_t) - 1u;
+  uint32_t s = hash_slot(j, log_t);
+  fresh = false;
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    int32_t k = keys[s];
+    if (k == j) return (int)s;
+    if (k == kEmpty) {
+      int32_t old = atomicCAS(&keys[s], kEmpty, j);
+      if (old == kEmpty) {
+        fresh = true;
+        return (int)s;
+      }
+      if (old == j) return (int)s;
+    }
+    s = (s + 1u) & mask;
+  }
+  raise_flag(flags, kFlagHashFull);
+  return -1;
+}
+
+// Looks up key j; returns its slot or -1.
+__device__ __forceinline__ int hash_find(const int32_t* keys, int log_t, int32_t j) {
+  const uint32_t mask = (1u << log_t) - 1u;
+  uint32_t s = hash_slot(j, log_t);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    int32_t k = keys[s];
+    if (k == j) return (int)s;
+    if (k == kEmpty) return -1;
+    s = (s + 1u) & mask;
+  }
+  return -1;
+}
+
+// Sorts n (key, value) pairs held in shared memory by key, using one warp
+// (bitonic network over next_pow2(n) <= cap slots; slots [n, np2) are filled
+// with +inf keys first).  Keys are distinct column indices.
+__device__ __forceinline__ void warp_sort_pairs(int32_t* keys, float* vals, int n, int cap) {
+  const int lane = lane_id();
+  int np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  if (np2 > cap) np2 = cap;  // caller guarantees np2 <= cap
+  for (int s = n + lane; s < np2; s += 32) keys[s] = 0x7fffffff;
+  __syncwarp();
+  for (int size = 2; size <= np2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = lane; i < (np2 >> 1); i += 32) {
+        // i-th compare pair: lo index has bit `stride` clear
+        int lo = ((i & ~(stride - 1)) << 1) | (i & (stride - 1));
+        int hi = lo | stride;
+        bool up = (lo & size) == 0;
+        int32_t a = keys[lo], b = keys[hi];
+        if ((a > b) == up) {
+          keys[lo] = b;
+          keys[hi] = a;
+          float va = vals[lo], vb = vals[hi];
+          vals[lo] = vb;
+          vals[hi] = va;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Key-only variant of warp_sort_pairs.
+__device__ __forceinline__ void warp_sort_keys(int32_t* keys, int n, int cap) {
+  const int lane = lane_id();
+  int np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  if (np2 > cap) np2 = cap;
+  for (int s = n + lane; s < np2; s += 32) keys[s] = 0x7fffffff;
+  __syncwarp();
+  for (int size = 2; size <= np2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = lane; i < (np2 >> 1); i += 32) {
+        int lo = ((i & ~(stride - 1)) << 1) | (i & (stride - 1));
+        int hi = lo | stride;
+        bool up = (lo & size) == 0;
+        int32_t a = keys[lo], b = keys[hi];
+        if ((a > b) == up) {
+          keys[lo] = b;
+          keys[hi] = a;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+}  // namespace spg

@@ -1,0 +1,78 @@
+// Host-side declarations of the SpGEMM kernel launchers.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace spg {
+
+struct DCsr;
+
+// Bin ids.  Warp-hash bins 0..7 hold tables of 2^(5+bin) slots.
+constexpr int kMinLogT = 5;
+constexpr int kMaxLogT = 12;
+constexpr int kNumWarpBins = kMaxLogT - kMinLogT + 1;  // 8
+constexpr int kBinBlock = 8;   // symbolic: CTA hash table
+constexpr int kBinDense = 9;   // symbolic: CTA bitmap over the column span
+constexpr int kBinHeavy = 10;  // numeric: column-tiled heavy rows
+constexpr int kBinEmpty = 11;  // no products
+constexpr int kNumBins = 12;
+
+constexpr int kBinSymbolic = 0;
+constexpr int kBinNumeric = 1;
+constexpr int kBinLearned = 2;
+
+constexpr int kTileWarps = 6;              // warps per CTA of the heavy tile kernel
+constexpr int kDenseWindowWords = 40960;   // 1,310,720 columns of bitmap per window
+
+struct BinParams {
+  int64_t warp_cap;    // largest bound (symbolic) / nnz (numeric) on a warp table
+  int64_t block_cap;   // largest bound on the symbolic CTA table
+  int warp_log_max;    // log2 of the largest warp table
+  float max_load;      // numeric table load factor
+};
+
+struct LaunchCtx {
+  cudaStream_t stream;
+  int sms;
+};
+
+void launch_widen_rp(const int32_t* in, int64_t n, int64_t* out, const LaunchCtx& lc);
+void launch_narrow_rp(const int64_t* in, int64_t n, int32_t* out, const LaunchCtx& lc);
+void launch_validate(const DCsr& M, int64_t nnz, int* flags, const LaunchCtx& lc);
+void launch_row_products(const DCsr& A, const DCsr& B, int64_t* prod, const LaunchCtx& lc);
+void launch_sum(const int64_t* v, int64_t n, unsigned long long* out, const LaunchCtx& lc);
+void launch_binning(const int64_t* key, int64_t rows, int64_t cols, int mode, const BinParams& bp,
+                    uint8_t* bin_of_row, int64_t* counts, int64_t* offsets, int64_t* cursors, int32_t* lists,
+                    const LaunchCtx& lc);
+int64_t scan_temp_elems(int64_t n);
+void launch_excl_scan(const int64_t* in, int64_t n, int64_t* out, int64_t* tmp, const LaunchCtx& lc);
+
+void launch_sym_warp(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int64_t* nnz,
+                     int* flags, const LaunchCtx& lc, int wpb);
+void launch_sym_block(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int log_table,
+                      int64_t slot_base, int64_t* nnz, int32_t* big_slot, int32_t* tile_cnt, int ntiles, int* flags,
+                      const LaunchCtx& lc);
+void launch_sym_dense(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int64_t slot_base,
+                      int64_t* nnz, int32_t* big_slot, int32_t* tile_cnt, int ntiles, int* flags,
+                      const LaunchCtx& lc);
+void launch_num_warp(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
+                     const int64_t* c_rp, int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb);
+void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
+                             const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
+                             int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
+                             const LaunchCtx& lc, int wpb);
+void launch_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot, const int32_t* tile_cnt,
+                         int ntiles, int32_t* tile_off, const LaunchCtx& lc);
+void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
+                     const int32_t* tile_cnt, const int32_t* tile_off, int ntiles, const int64_t* c_rp,
+                     int32_t* c_col, float* c_val, unsigned long long* tile_counter, int* flags,
+                     const LaunchCtx& lc);
+void launch_compact_rows(const int32_t* rows, int64_t nrows, const uint8_t* need_exact, const int64_t* slab_off,
+                         const int32_t* slab_col, const float* slab_val, const int64_t* c_rp, int32_t* c_col,
+                         float* c_val, const LaunchCtx& lc);
+void launch_mark_rows(const int32_t* retry, const unsigned long long* count, uint8_t* need_exact, const LaunchCtx& lc);
+void launch_mask_key(const int64_t* src, const uint8_t* mask, int64_t rows, int64_t* dst, const LaunchCtx& lc);
+
+}  // namespace spg

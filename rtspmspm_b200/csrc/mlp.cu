@@ -1,0 +1,422 @@
+// Learned row-size predictor: feature kernel, inference kernel and the
+// training kernels (forward + backward + Adam) of an 8 -> 64 -> 64 -> 2 MLP
+// with BF16 weights and FP32 accumulation.
+//
+// No reference counterpart: the reference sizes its output as a dense
+// rows x cols buffer (optixSpMSpM/src/optixSpMSpM/optixSpMSpM.cpp:164-171)
+// and never predicts row sizes.  The predictor replaces the symbolic pass
+// for rows whose predicted size is trusted; overflowing rows are re-run by
+// the exact path, so results never depend on the network.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "mlp.hpp"
+
+namespace spg {
+
+// Feature scaling: every feature is a log2 quantity divided by 16.
+constexpr float kFeatScale = 1.0f / 16.0f;
+
+// Features of row r of A*B (one warp per row):
+//  0 log2(1 + |A_r|)               4 log2(1 + cols of B)
+//  1 log2(1 + products)            5 log2(1 + output column span)
+//  2 log2(1 + max touched |B_k|)   6 distinct fraction of a 32-product sample
+//  3 log2(1 + min touched |B_k|)   7 log2(1 + cols (1 - exp(-products/cols)))
+// Also writes the products (int64) of the row.
+__global__ void k_features(DCsr A, DCsr B, float* feats, int64_t* prod) {
+  const int lane = lane_id();
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = gw; r < A.rows; r += nw) {
+    const int64_t s = A.rp[r], e = A.rp[r + 1];
+    const int64_t len = e - s;
+    int64_t sum = 0, mx = 0, mn = INT64_MAX;
+    int lo = 0x7fffffff, hi = -1;
+    for (int64_t p = s + lane; p < e; p += 32) {
+      const int32_t k = A.col[p];
+      const int64_t bs = B.rp[k], be = B.rp[k + 1];
+      const int64_t l = be - bs;
+      sum += l;
+      mx = l > mx ? l : mx;
+      mn = l < mn ? l : mn;
+      if (l > 0) {
+        lo = min(lo, B.col[bs]);
+        hi = max(hi, B.col[be - 1]);
+      }
+    }
+    sum = warp_sum(sum);
+    mx = warp_max(mx);
+    mn = warp_min(mn);
+    lo = warp_min(lo);
+    hi = warp_max(hi);
+    // sample: lane l takes A entry s + l*len/32 and the middle of its B row
+    int32_t j = -1 - lane;
+    bool valid = false;
+    if (len > 0 && lane < len) {
+      const int64_t p = s + (len <= 32 ? lane : (int64_t)lane * len / 32);
+      const int32_t k = A.col[p];
+      const int64_t bs = B.rp[k], be = B.rp[k + 1];
+      if (be > bs) {
+        const uint32_t hsh = (uint32_t)r * 2654435761u + (uint32_t)lane * 40503u;
+        j = B.col[bs + (int64_t)(hsh % (uint32_t)(be - bs))];
+        valid = true;
+      }
+    }
+    const unsigned vm = __ballot_sync(kFull, valid);
+    const unsigned grp = __match_any_sync(kFull, j);
+    const bool leader = valid && lane == __ffs(grp & vm) - 1;
+    const int distinct = __popc(__ballot_sync(kFull, leader));
+    const int nsample = __popc(vm);
+    if (lane == 0) {
+      if (mn == INT64_MAX) mn = 0;
+      const double cols = (double)B.cols;
+      const double span = hi >= lo ? (double)(hi - lo + 1) : 0.0;
+      const double expect = cols > 0 ? cols * (1.0 - exp(-(double)sum / cols)) : 0.0;
+      float* f = feats + r * kMlpIn;
+      f[0] = log2f(1.f + (float)len) * kFeatScale;
+      f[1] = (float)log2(1.0 + (double)sum) * kFeatScale;
+      f[2] = log2f(1.f + (float)mx) * kFeatScale;
+      f[3] = log2f(1.f + (float)mn) * kFeatScale;
+      f[4] = (float)log2(1.0 + cols) * kFeatScale;
+      f[5] = (float)log2(1.0 + span) * kFeatScale;
+      f[6] = nsample ? (float)distinct / (float)nsample : 0.f;
+      f[7] = (float)log2(1.0 + expect) * kFeatScale;
+      if (prod) prod[r] = sum;
+    }
+  }
+}
+
+// Parameter offsets inside the flat parameter vector.
+constexpr int kOffW1 = 0;
+constexpr int kOffB1 = kOffW1 + kMlpIn * kMlpHidden;
+constexpr int kOffW2 = kOffB1 + kMlpHidden;
+constexpr int kOffB2 = kOffW2 + kMlpHidden * kMlpHidden;
+constexpr int kOffW3 = kOffB2 + kMlpHidden;
+constexpr int kOffB3 = kOffW3 + kMlpHidden * kMlpOut;
+static_assert(kOffB3 + kMlpOut == kMlpParams, "parameter layout");
+
+// Loads the BF16 parameters (weights and biases) into shared memory as FP32.
+__device__ __forceinline__ void load_params(const __nv_bfloat16* w, float* sw) {
+  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) sw[i] = __bfloat162float(w[i]);
+  __syncthreads();
+}
+
+// Forward pass of one row; h1 kept in registers, h2 streamed into the output.
+// `sw` is read through a volatile pointer so the compiler re-reads the
+// weights per row instead of hoisting all 4,736 of them into registers.
+__device__ __forceinline__ void mlp_forward_row(const volatile float* sw, const float* x, float* h1, float* out) {
+#pragma unroll
+  for (int j = 0; j < kMlpHidden; ++j) {
+    float a = sw[kOffB1 + j];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; ++i) a += x[i] * sw[kOffW1 + i * kMlpHidden + j];
+    h1[j] = a > 0.f ? a : 0.f;
+  }
+  float o0 = sw[kOffB3 + 0], o1 = sw[kOffB3 + 1];
+#pragma unroll 1
+  for (int j = 0; j < kMlpHidden; ++j) {
+    float a = sw[kOffB2 + j];
+#pragma unroll
+    for (int i = 0; i < kMlpHidden; ++i) a += h1[i] * sw[kOffW2 + i * kMlpHidden + j];
+    a = a > 0.f ? a : 0.f;
+    o0 += a * sw[kOffW3 + j * kMlpOut + 0];
+    o1 += a * sw[kOffW3 + j * kMlpOut + 1];
+  }
+  out[0] = o0;
+  out[1] = o1;
+}
+
+// Inference: predicted log2(1+nnz) and bin per row.
+__global__ void k_mlp_predict(const __nv_bfloat16* w, const float* feats, int64_t rows, float* out) {
+  extern __shared__ float sw[];
+  load_params(w, sw);
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    float x[kMlpIn], h1[kMlpHidden], o[kMlpOut];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; ++i) x[i] = feats[r * kMlpIn + i];
+    mlp_forward_row(sw, x, h1, o);
+    out[r * kMlpOut + 0] = o[0];
+    out[r * kMlpOut + 1] = o[1];
+  }
+}
+
+// Inference fused with capacity sizing for the learned SpGEMM path.
+// cap = min(bound, ceil(margin * (2^o0 - 1)) + slack); a row is sent to the
+// exact path (need_exact = 1, cap = 0) when its cap exceeds the largest warp
+// table, its predicted bin says heavy, or force_overflow is set (cap = 1).
+__global__ void k_mlp_capacity(const __nv_bfloat16* w, const float* feats, const int64_t* prod, int64_t rows,
+                               int64_t cols, float margin, int slack, int64_t warp_cap, int force_overflow,
+                               int64_t* cap, uint8_t* need_exact) {
+  extern __shared__ float sw[];
+  load_params(w, sw);
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = prod[r];
+    const int64_t u = p < cols ? p : cols;
+    int64_t c = 0;
+    uint8_t ex = 0;
+    if (u > 0) {
+      float x[kMlpIn], h1[kMlpHidden], o[kMlpOut];
+#pragma unroll
+      for (int i = 0; i < kMlpIn; ++i) x[i] = feats[r * kMlpIn + i];
+      mlp_forward_row(sw, x, h1, o);
+      const float lg = fminf(fmaxf(o[0], 0.f), 40.f);
+      double pred = exp2((double)lg) - 1.0;
+      double cd = ceil(pred * (double)margin) + (double)slack;
+      c = cd >= (double)u ? u : (int64_t)cd;
+      if (c < 1) c = 1;
+      if (force_overflow) c = 1;
+      if (c > warp_cap || o[1] > (float)(kMaxLogT + 0.5f)) {
+        ex = 1;
+        c = 0;
+      }
+    }
+    cap[r] = c;
+    need_exact[r] = ex;
+  }
+}
+
+// Training, step 1 of 3 (one thread per row of the minibatch): forward
+// with BF16 weights; keeps h1, z2 and dL/do for the backward kernels.
+// Loss = 0.5 * mean over rows of sum_o w_o (y_o - t_o)^2 with w = (1, 1/4).
+constexpr int kTrainThreads = 128;
+constexpr float kLossW0 = 1.0f;
+constexpr float kLossW1 = 0.25f;
+
+__global__ void __launch_bounds__(kTrainThreads) k_mlp_fwd(const __nv_bfloat16* w, const float* feats,
+                                                             const float* targets, int64_t n, float inv_n,
+                                                             float* h1_out, float* z2_out, float* do_out,
+                                                             float* loss_rows) {
+  extern __shared__ float sw[];
+  load_params(w, sw);
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    const volatile float* vw = sw;
+    float x[kMlpIn], h1[kMlpHidden];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; ++i) x[i] = feats[r * kMlpIn + i];
+#pragma unroll
+    for (int j = 0; j < kMlpHidden; ++j) {
+      float a = vw[kOffB1 + j];
+#pragma unroll
+      for (int i = 0; i < kMlpIn; ++i) a += x[i] * vw[kOffW1 + i * kMlpHidden + j];
+      h1[j] = a > 0.f ? a : 0.f;
+      h1_out[r * kMlpHidden + j] = h1[j];
+    }
+    float o0 = vw[kOffB3], o1 = vw[kOffB3 + 1];
+#pragma unroll 1
+    for (int j = 0; j < kMlpHidden; ++j) {
+      float a = vw[kOffB2 + j];
+#pragma unroll
+      for (int i = 0; i < kMlpHidden; ++i) a += h1[i] * vw[kOffW2 + i * kMlpHidden + j];
+      z2_out[r * kMlpHidden + j] = a;
+      const float h = a > 0.f ? a : 0.f;
+      o0 += h * vw[kOffW3 + j * kMlpOut + 0];
+      o1 += h * vw[kOffW3 + j * kMlpOut + 1];
+    }
+    const float e0 = o0 - targets[r * kMlpOut + 0];
+    const float e1 = o1 - targets[r * kMlpOut + 1];
+    do_out[r * kMlpOut + 0] = kLossW0 * e0 * inv_n;
+    do_out[r * kMlpOut + 1] = kLossW1 * e1 * inv_n;
+    loss_rows[r] = 0.5f * (kLossW0 * e0 * e0 + kLossW1 * e1 * e1);
+  }
+}
+
+// Training, step 2 of 3 (one thread per row): back-propagates dL/do into
+// dL/dz2 and dL/dz1 (pre-activation gradients of both hidden layers).
+__global__ void __launch_bounds__(kTrainThreads) k_mlp_bwd_rows(const __nv_bfloat16* w, int64_t n, const float* h1_in,
+                                                                  const float* z2_in, const float* do_in,
+                                                                  float* dz1_out, float* dz2_out) {
+  extern __shared__ float sw[];
+  load_params(w, sw);
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    const volatile float* vw = sw;
+    const float d0 = do_in[r * kMlpOut + 0], d1 = do_in[r * kMlpOut + 1];
+    float dh1[kMlpHidden];
+#pragma unroll
+    for (int i = 0; i < kMlpHidden; ++i) dh1[i] = 0.f;
+#pragma unroll 1
+    for (int j = 0; j < kMlpHidden; ++j) {
+      const float z = z2_in[r * kMlpHidden + j];
+      const float dz = z > 0.f ? d0 * vw[kOffW3 + j * kMlpOut + 0] + d1 * vw[kOffW3 + j * kMlpOut + 1] : 0.f;
+      dz2_out[r * kMlpHidden + j] = dz;
+#pragma unroll
+      for (int i = 0; i < kMlpHidden; ++i) dh1[i] += dz * vw[kOffW2 + i * kMlpHidden + j];
+    }
+#pragma unroll
+    for (int i = 0; i < kMlpHidden; ++i)
+      dz1_out[r * kMlpHidden + i] = h1_in[r * kMlpHidden + i] > 0.f ? dh1[i] : 0.f;
+  }
+}
+
+// Training, step 3 of 3 (one thread per parameter): each gradient is a sum
+// over the minibatch rows in row order -- deterministic, no atomics.
+__global__ void k_mlp_grad_reduce(const float* feats, int64_t n, const float* h1, const float* z2, const float* d_o,
+                                  const float* dz1, const float* dz2, float* grad) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kMlpParams) return;
+  float g = 0.f;
+  if (p < kOffB1) {  // W1[f][i]
+    const int f = (p - kOffW1) / kMlpHidden, i = (p - kOffW1) % kMlpHidden;
+    for (int64_t r = 0; r < n; ++r) g += feats[r * kMlpIn + f] * dz1[r * kMlpHidden + i];
+  } else if (p < kOffW2) {  // b1[i]
+    const int i = p - kOffB1;
+    for (int64_t r = 0; r < n; ++r) g += dz1[r * kMlpHidden + i];
+  } else if (p < kOffB2) {  // W2[i][j]
+    const int i = (p - kOffW2) / kMlpHidden, j = (p - kOffW2) % kMlpHidden;
+    for (int64_t r = 0; r < n; ++r) g += h1[r * kMlpHidden + i] * dz2[r * kMlpHidden + j];
+  } else if (p < kOffW3) {  // b2[j]
+    const int j = p - kOffB2;
+    for (int64_t r = 0; r < n; ++r) g += dz2[r * kMlpHidden + j];
+  } else if (p < kOffB3) {  // W3[j][k]
+    const int j = (p - kOffW3) / kMlpOut, k = (p - kOffW3) % kMlpOut;
+    for (int64_t r = 0; r < n; ++r) {
+      const float z = z2[r * kMlpHidden + j];
+      g += (z > 0.f ? z : 0.f) * d_o[r * kMlpOut + k];
+    }
+  } else {  // b3[k]
+    const int k = p - kOffB3;
+    for (int64_t r = 0; r < n; ++r) g += d_o[r * kMlpOut + k];
+  }
+  grad[p] = g;
+}
+
+// Sum of per-row losses divided by n (single CTA, fixed order per thread).
+__global__ void k_loss_mean(const float* loss_rows, int64_t n, float inv_n, float* out) {
+  __shared__ float sh[32];
+  float s = 0.f;
+  for (int64_t r = threadIdx.x; r < n; r += blockDim.x) s += loss_rows[r];
+  s = warp_sum(s);
+  if (lane_id() == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.f;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) *out = v * inv_n;
+  }
+}
+
+// Adam with decoupled weight decay on the FP32 master weights; refreshes
+// the BF16 copy used by the forward kernels.
+__global__ void k_adam(float* master, __nv_bfloat16* w16, float* grad, float* m, float* v, int n, float lr,
+                       float beta1, float beta2, float eps, float wd, float bc1, float bc2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float g = grad[i];
+    const float mi = beta1 * m[i] + (1.f - beta1) * g;
+    const float vi = beta2 * v[i] + (1.f - beta2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    float p = master[i];
+    p -= lr * ((mi / bc1) / (sqrtf(vi / bc2) + eps) + wd * p);
+    master[i] = p;
+    w16[i] = __float2bfloat16_rn(p);
+  }
+}
+
+__global__ void k_to_bf16(const float* src, __nv_bfloat16* dst, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dst[i] = __float2bfloat16_rn(src[i]);
+}
+
+// Training targets from exact nnz: t0 = log2(1 + nnz), t1 = numeric bin as
+// log2 of the warp table size (kMaxLogT + 1 for heavy rows).
+__global__ void k_make_targets(const int64_t* nnz, const int32_t* idx, int64_t n, float max_load, int64_t warp_cap,
+                               float* targets) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = nnz[idx ? idx[t] : t];
+    float b;
+    if (v <= 0) b = (float)kMinLogT;
+    else if (v > warp_cap) b = (float)(kMaxLogT + 1);
+    else {
+      int64_t need = (int64_t)ceilf((float)v / max_load);
+      int lg = need <= 1 ? 0 : 64 - __clzll((unsigned long long)(need - 1));
+      if (lg < kMinLogT) lg = kMinLogT;
+      if (lg > kMaxLogT) lg = kMaxLogT;
+      b = (float)lg;
+    }
+    targets[t * 2 + 0] = (float)log2(1.0 + (double)v);
+    targets[t * 2 + 1] = b;
+  }
+}
+
+// Gathers rows idx[0..n) of a rows x width float matrix.
+__global__ void k_gather_rows(const float* src, const int32_t* idx, int64_t n, int width, float* dst) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * width; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = t / width;
+    dst[t] = src[(int64_t)idx[r] * width + (t % width)];
+  }
+}
+
+// --------------------------------------------------------------------------
+
+void launch_features(const DCsr& A, const DCsr& B, float* feats, int64_t* prod, const LaunchCtx& lc) {
+  if (A.rows == 0) return;
+  int64_t blocks = (A.rows * 32 + 255) / 256;
+  if (blocks > lc.sms * 16) blocks = lc.sms * 16;
+  k_features<<<(unsigned)blocks, 256, 0, lc.stream>>>(A, B, feats, prod);
+}
+
+static int mlp_blocks(int64_t rows, int threads, int sms) {
+  int64_t b = (rows + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > sms * 8) b = sms * 8;
+  return (int)b;
+}
+
+void launch_mlp_predict(const void* w16, const float* feats, int64_t rows, float* out, const LaunchCtx& lc) {
+  if (rows == 0) return;
+  k_mlp_predict<<<mlp_blocks(rows, 128, lc.sms), 128, kMlpParams * sizeof(float), lc.stream>>>(
+      (const __nv_bfloat16*)w16, feats, rows, out);
+}
+
+void launch_mlp_capacity(const void* w16, const float* feats, const int64_t* prod, int64_t rows, int64_t cols,
+                         float margin, int slack, int64_t warp_cap, int force_overflow, int64_t* cap,
+                         uint8_t* need_exact, const LaunchCtx& lc) {
+  if (rows == 0) return;
+  k_mlp_capacity<<<mlp_blocks(rows, 128, lc.sms), 128, kMlpParams * sizeof(float), lc.stream>>>(
+      (const __nv_bfloat16*)w16, feats, prod, rows, cols, margin, slack, warp_cap, force_overflow, cap, need_exact);
+}
+
+void launch_mlp_fwd_bwd(const void* w16, const float* feats, const float* targets, int64_t n, float* work,
+                        float* grad, float* loss, const LaunchCtx& lc) {
+  if (n == 0) return;
+  float* h1 = work;
+  float* z2 = h1 + n * kMlpHidden;
+  float* dz1 = z2 + n * kMlpHidden;
+  float* dz2 = dz1 + n * kMlpHidden;
+  float* d_o = dz2 + n * kMlpHidden;
+  float* lrows = d_o + n * kMlpOut;
+  const int blocks = mlp_blocks(n, kTrainThreads, lc.sms);
+  const size_t smem = kMlpParams * sizeof(float);
+  const float inv_n = 1.0f / (float)n;
+  k_mlp_fwd<<<blocks, kTrainThreads, smem, lc.stream>>>((const __nv_bfloat16*)w16, feats, targets, n, inv_n, h1, z2,
+                                                        d_o, lrows);
+  k_mlp_bwd_rows<<<blocks, kTrainThreads, smem, lc.stream>>>((const __nv_bfloat16*)w16, n, h1, z2, d_o, dz1, dz2);
+  k_mlp_grad_reduce<<<(kMlpParams + 127) / 128, 128, 0, lc.stream>>>(feats, n, h1, z2, d_o, dz1, dz2, grad);
+  if (loss) k_loss_mean<<<1, 1024, 0, lc.stream>>>(lrows, n, inv_n, loss);
+}
+
+int64_t mlp_work_floats(int64_t n) { return n * (4 * kMlpHidden + kMlpOut + 1); }
+
+void launch_adam(float* master, void* w16, float* grad, float* m, float* v, float lr, float beta1, float beta2,
+                 float eps, float wd, int step, const LaunchCtx& lc) {
+  const float bc1 = 1.f - powf(beta1, (float)step);
+  const float bc2 = 1.f - powf(beta2, (float)step);
+  k_adam<<<(kMlpParams + 255) / 256, 256, 0, lc.stream>>>(master, (__nv_bfloat16*)w16, grad, m, v, kMlpParams, lr,
+                                                          beta1, beta2, eps, wd, bc1, bc2);
+}
+
+void launch_to_bf16(const float* src, void* dst, int n, const LaunchCtx& lc) {
+  k_to_bf16<<<(n + 255) / 256, 256, 0, lc.stream>>>(src, (__nv_bfloat16*)dst, n);
+}
+
+void launch_make_targets(const int64_t* nnz, const int32_t* idx, int64_t n, float max_load, int64_t warp_cap,
+                         float* targets, const LaunchCtx& lc) {
+  if (n == 0) return;
+  k_make_targets<<<mlp_blocks(n, 256, lc.sms), 256, 0, lc.stream>>>(nnz, idx, n, max_load, warp_cap, targets);
+}
+
+void launch_gather_rows(const float* src, const int32_t* idx, int64_t n, int width, float* dst, const LaunchCtx& lc) {
+  if (n == 0) return;
+  k_gather_rows<<<mlp_blocks(n * width, 256, lc.sms), 256, 0, lc.stream>>>(src, idx, n, width, dst);
+}
+
+}  // namespace spg

@@ -1,0 +1,282 @@
+// Matrix Market reader / writer of the C ABI (host code).
+//
+// Reader: replaces the reference's three line-by-line istringstream parsers
+// (cooFromFile cuSparse/src/util.cpp:9-44, mat1ToGPU
+// optixSpMSpM/src/optixSpMSpM/optixSpMSpM.cpp:73-131, Sphere::Sphere
+// optixSpMSpM/src/optixSpMSpM/Sphere.cpp:26-78).  The whole file is read
+// at once and parsed with std::from_chars; entries may come in any order
+// (the shipped fixtures are column-major), are converted to 0-based CSR with
+// sorted columns, and duplicate (i, j) pairs are summed in FP32 in file
+// order.  `symmetric` files are expanded; `pattern` files get value 1.
+//
+// Writer: the reference's two writers -- printCooToFile
+// (cuSparse/src/util.cpp:49-69, every structural entry) and printResult
+// (optixSpMSpM.cpp:452-494, row-major, skips exact zeros).  Lines are
+// `i j v`, 1-based, row-major with ascending columns; values use the
+// shortest decimal form that reads back to the same FP32.
+#include <algorithm>
+#include <charconv>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/rtspmspm.h"
+
+namespace {
+
+struct Cursor {
+  const char* p;
+  const char* end;
+  bool at_end() const { return p >= end; }
+  void skip_blank() {
+    while (p < end && (*p == ' ' || *p == '\t' || *p == '\r')) ++p;
+  }
+  void next_line() {
+    while (p < end && *p != '\n') ++p;
+    if (p < end) ++p;
+  }
+  template <typename T>
+  bool read_int(T& v) {
+    skip_blank();
+    auto r = std::from_chars(p, end, v);
+    if (r.ec != std::errc()) return false;
+    p = r.ptr;
+    return true;
+  }
+  bool read_float(float& v) {
+    skip_blank();
+    // accept a leading '+' which from_chars rejects
+    if (p < end && *p == '+') ++p;
+    auto r = std::from_chars(p, end, v);
+    if (r.ec == std::errc::result_out_of_range) {
+      // denormal / overflow literals: fall back to strtof semantics
+      char buf[64];
+      size_t n = std::min<size_t>(63, (size_t)(r.ptr - p));
+      std::memcpy(buf, p, n);
+      buf[n] = 0;
+      v = std::strtof(buf, nullptr);
+      p = r.ptr;
+      return true;
+    }
+    if (r.ec != std::errc()) return false;
+    p = r.ptr;
+    return true;
+  }
+};
+
+bool read_file(const char* path, std::vector<char>& buf) {
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return false;
+  std::fseek(f, 0, SEEK_END);
+  long n = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
+  if (n < 0) {
+    std::fclose(f);
+    return false;
+  }
+  buf.resize((size_t)n);
+  size_t got = n ? std::fread(buf.data(), 1, (size_t)n, f) : 0;
+  std::fclose(f);
+  return got == (size_t)n;
+}
+
+std::string lower(std::string s) {
+  for (auto& c : s) c = (char)std::tolower((unsigned char)c);
+  return s;
+}
+
+}  // namespace
+
+extern "C" spg_status spg_mtx_read(const char* path, spg_csr* out) {
+  if (!path || !out) return SPG_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof *out);
+  std::vector<char> buf;
+  if (!read_file(path, buf)) return SPG_ERR_IO;
+  Cursor c{buf.data(), buf.data() + buf.size()};
+  bool pattern = false, symmetric = false, skew = false;
+  // banner (optional) and comments
+  if (buf.size() >= 2 && buf[0] == '%' && buf[1] == '%') {
+    const char* e = c.p;
+    while (e < c.end && *e != '\n') ++e;
+    std::string banner = lower(std::string(c.p, e));
+    if (banner.find("coordinate") == std::string::npos) return SPG_ERR_FORMAT;
+    if (banner.find("complex") != std::string::npos) return SPG_ERR_UNSUPPORTED;
+    pattern = banner.find("pattern") != std::string::npos;
+    symmetric = banner.find("symmetric") != std::string::npos || banner.find("hermitian") != std::string::npos;
+    skew = banner.find("skew-symmetric") != std::string::npos;
+    c.next_line();
+  }
+  while (!c.at_end()) {
+    c.skip_blank();
+    if (c.at_end()) break;
+    if (*c.p == '%' || *c.p == '\n') {
+      c.next_line();
+      continue;
+    }
+    break;
+  }
+  int64_t rows = 0, cols = 0, nnz = 0;
+  if (!c.read_int(rows) || !c.read_int(cols) || !c.read_int(nnz)) return SPG_ERR_FORMAT;
+  if (rows < 0 || cols < 0 || nnz < 0 || cols > INT32_MAX || rows > INT32_MAX) return SPG_ERR_FORMAT;
+  c.next_line();
+  const int64_t cap = symmetric ? 2 * nnz : nnz;
+  std::vector<int32_t> ri, ci;
+  std::vector<float> vv;
+  ri.reserve((size_t)cap);
+  ci.reserve((size_t)cap);
+  vv.reserve((size_t)cap);
+  int64_t seen = 0;
+  while (seen < nnz) {
+    c.skip_blank();
+    if (c.at_end()) return SPG_ERR_FORMAT;
+    if (*c.p == '\n' || *c.p == '%') {
+      c.next_line();
+      continue;
+    }
+    int64_t i = 0, j = 0;
+    float v = 1.0f;
+    if (!c.read_int(i) || !c.read_int(j)) return SPG_ERR_FORMAT;
+    if (!pattern && !c.read_float(v)) return SPG_ERR_FORMAT;
+    if (i < 1 || i > rows || j < 1 || j > cols) return SPG_ERR_FORMAT;
+    ri.push_back((int32_t)(i - 1));
+    ci.push_back((int32_t)(j - 1));
+    vv.push_back(v);
+    if (symmetric && i != j) {
+      ri.push_back((int32_t)(j - 1));
+      ci.push_back((int32_t)(i - 1));
+      vv.push_back(skew ? -v : v);
+    }
+    ++seen;
+    c.next_line();
+  }
+  // counting sort by row (stable: keeps file order inside a row)
+  const size_t m = ri.size();
+  std::vector<int64_t> rp((size_t)rows + 1, 0);
+  for (size_t t = 0; t < m; ++t) ++rp[(size_t)ri[t] + 1];
+  for (int64_t r = 0; r < rows; ++r) rp[(size_t)r + 1] += rp[(size_t)r];
+  std::vector<int64_t> pos(rp.begin(), rp.end() - 1);
+  std::vector<int32_t> col(m);
+  std::vector<float> val(m);
+  for (size_t t = 0; t < m; ++t) {
+    const int64_t d = pos[(size_t)ri[t]]++;
+    col[(size_t)d] = ci[t];
+    val[(size_t)d] = vv[t];
+  }
+  ri.clear();
+  ri.shrink_to_fit();
+  ci.clear();
+  ci.shrink_to_fit();
+  vv.clear();
+  vv.shrink_to_fit();
+  // sort columns per row (stable), merge duplicates in file order
+  std::vector<int64_t> orp((size_t)rows + 1, 0);
+  std::vector<std::pair<int32_t, float>> tmp;
+  int64_t w = 0;
+  for (int64_t r = 0; r < rows; ++r) {
+    const int64_t s = rp[(size_t)r], e = rp[(size_t)r + 1];
+    tmp.assign(e - s, {});
+    for (int64_t t = s; t < e; ++t) tmp[(size_t)(t - s)] = {col[(size_t)t], val[(size_t)t]};
+    std::stable_sort(tmp.begin(), tmp.end(),
+                     [](const std::pair<int32_t, float>& a, const std::pair<int32_t, float>& b) {
+                       return a.first < b.first;
+                     });
+    for (size_t t = 0; t < tmp.size(); ++t) {
+      if (t > 0 && tmp[t].first == tmp[t - 1].first) {
+        val[(size_t)(w - 1)] = val[(size_t)(w - 1)] + tmp[t].second;
+      } else {
+        col[(size_t)w] = tmp[t].first;
+        val[(size_t)w] = tmp[t].second;
+        ++w;
+      }
+    }
+    orp[(size_t)r + 1] = w;
+  }
+  const size_t rpb = ((size_t)rows + 1) * sizeof(int64_t);
+  int64_t* hrp = (int64_t*)std::malloc(rpb);
+  int32_t* hcol = (int32_t*)std::malloc(std::max<size_t>((size_t)w * 4, 4));
+  float* hval = (float*)std::malloc(std::max<size_t>((size_t)w * 4, 4));
+  if (!hrp || !hcol || !hval) {
+    std::free(hrp);
+    std::free(hcol);
+    std::free(hval);
+    return SPG_ERR_OUT_OF_MEMORY;
+  }
+  std::memcpy(hrp, orp.data(), rpb);
+  if (w) {
+    std::memcpy(hcol, col.data(), (size_t)w * 4);
+    std::memcpy(hval, val.data(), (size_t)w * 4);
+  }
+  out->rows = rows;
+  out->cols = cols;
+  out->nnz = w;
+  out->capacity = w;
+  out->index_bits = 64;
+  out->location = SPG_HOST;
+  out->row_ptr = hrp;
+  out->col_idx = hcol;
+  out->val = hval;
+  out->owner = 2;
+  return SPG_OK;
+}
+
+extern "C" spg_status spg_mtx_write(spg_ctx* ctx, const char* path, const spg_csr* m, int32_t drop_zeros) {
+  if (!path || !m) return SPG_ERR_INVALID_ARG;
+  spg_csr host{};
+  const spg_csr* src = m;
+  if (m->location == SPG_DEVICE) {
+    if (!ctx) return SPG_ERR_INVALID_ARG;
+    spg_status st = spg_csr_copy(ctx, m, SPG_HOST, &host);
+    if (st != SPG_OK) return st;
+    src = &host;
+  }
+  auto rp_at = [&](int64_t r) -> int64_t {
+    return src->index_bits == 64 ? static_cast<const int64_t*>(src->row_ptr)[r]
+                                 : (int64_t) static_cast<const int32_t*>(src->row_ptr)[r];
+  };
+  int64_t count = 0;
+  if (drop_zeros) {
+    for (int64_t t = 0; t < src->nnz; ++t) count += src->val[t] != 0.0f;
+  } else {
+    count = src->nnz;
+  }
+  FILE* f = std::fopen(path, "wb");
+  if (!f) {
+    spg_csr_free(ctx, &host);
+    return SPG_ERR_IO;
+  }
+  std::fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n%lld %lld %lld\n", (long long)src->rows,
+               (long long)src->cols, (long long)count);
+  std::vector<char> out;
+  out.reserve(1 << 22);
+  char tmp[64];
+  bool ok = true;
+  for (int64_t r = 0; r < src->rows && ok; ++r) {
+    const int64_t s = rp_at(r), e = rp_at(r + 1);
+    for (int64_t t = s; t < e; ++t) {
+      const float v = src->val[t];
+      if (drop_zeros && v == 0.0f) continue;
+      char* p = tmp;
+      p = std::to_chars(p, tmp + sizeof tmp, r + 1).ptr;
+      *p++ = ' ';
+      p = std::to_chars(p, tmp + sizeof tmp, (int64_t)src->col_idx[t] + 1).ptr;
+      *p++ = ' ';
+      p = std::to_chars(p, tmp + sizeof tmp, v).ptr;
+      *p++ = '\n';
+      out.insert(out.end(), tmp, p);
+      if (out.size() > (1 << 22) - 64) {
+        ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+        out.clear();
+      }
+    }
+  }
+  if (ok && !out.empty()) ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+  ok = (std::fclose(f) == 0) && ok;
+  spg_csr_free(ctx, &host);
+  return ok ? SPG_OK : SPG_ERR_IO;
+}

@@ -1,0 +1,368 @@
+"""Benchmark: C = A*A on the 27-point stencil over a 96^3 grid (884,736 rows,
+23.4M nonzeros), learned-binned SpGEMM vs the plain two-pass method on one
+B200, through the library's C ABI.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full C = A*A (validation off, C allocated and released by the
+library), inputs resident in HBM.  Timed with CUDA events on the stream the
+library launches on, L2 flushed between steps; under torchrun every rank runs
+its own replica and the slowest rank's time counts (weak scaling).  Rank 0
+prints one JSON line.
+
+--impl reference times the reference arm on the host cores: the reference
+has no CPU SpMSpM path, so the arm is the CPU restatement of its arithmetic
+(oracle/spgemm_oracle.c, OpenMP, canonical FP32 order) on a bounded row
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SpGEMM GFLOP/s & ms per C=A·A, learned-binned vs plain 2-pass on same B200"
+WORKLOAD = "C=A*A, A = 27-point 3D stencil on a 96^3 grid (884,736 rows), FP32 N(0,1), diag 26+sum|row|"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def csr_bytes(rows, nnz, rp_bytes=4):
+    return nnz * 8 + (rows + 1) * rp_bytes
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAKS_FALLBACK["hbm_gbs"], "fallback"
+
+
+def traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` on this workload, from the committed
+    ncu summary (profiles/traffic.txt: `<kernel> <workload> <bytes>`)."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 3 and parts[0] == kernel and parts[1] == "stencil96":
+                    return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        # one synchronous query first: nvidia-smi's first start-up is slow and
+        # must not land inside the timed region
+        subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm", "--format=csv"],
+                       capture_output=True, timeout=60)
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 4 + i and s[4 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_sample(A, target_s: float, threads: int | None = None):
+    """Times the oracle (FP32 canonical Gustavson, OpenMP) on leading rows of A*A,
+    sized to about target_s seconds.  Returns (GFLOP/s, dict)."""
+    from oracle import oracle
+    from rtspmspm_b200 import gen
+
+    if threads:
+        oracle.set_threads(threads)
+    cores = oracle.num_threads()
+    prod = gen.row_products(A, A)
+    cum = np.cumsum(prod)
+    # calibrate on ~0.5% of the work, then size the sample
+    r1 = int(np.searchsorted(cum, cum[-1] * 0.005)) + 1
+    t = time.perf_counter()
+    oracle.baseline_rows(A, A, 0, r1)
+    dt = max(time.perf_counter() - t, 1e-4)
+    rate = float(cum[r1 - 1]) / dt
+    want = min(float(cum[-1]), rate * target_s)
+    r2 = int(np.searchsorted(cum, want)) + 1
+    r2 = min(r2, A.rows)
+    t = time.perf_counter()
+    oracle.baseline_rows(A, A, 0, r2)
+    dt = time.perf_counter() - t
+    work = float(cum[r2 - 1])
+    return 2.0 * work / dt / 1e9, {"cores": cores, "rows": r2, "products": int(work), "seconds": dt}
+
+
+def reference_arm(args, A):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    vals = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        v, info = cpu_sample(A, per_step)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    sample = f"leading {info['rows']} rows of the stencil-96 C=A*A ({info['products']} products, " \
+             f"{info['seconds']:.1f} s per step)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GFLOP/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(info["seconds"] * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": "bounded row sample"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=96)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", choices=["plain", "learned"], default=None,
+                    help="only W warm-up + K steps of one method (short runs under ncu)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    from rtspmspm_b200 import gen
+
+    A = gen.stencil27(args.grid, seed=0)
+    if args.impl == "reference":
+        return reference_arm(args, A)
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from rtspmspm_b200 import DeviceCsr, Engine, HostCsr, _lib
+
+    eng = Engine(local, use_torch_stream=True)
+    stream = torch.cuda.current_stream()
+    dA = DeviceCsr.from_host(A, device=local, index_bits=32)
+    products = int(gen.row_products(A, A).sum())
+    flops = 2.0 * products
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sa = dA.struct()
+
+    def run_steps(algo: str, k: int, stage_timing=False):
+        """k timed steps; returns (ms per step, last report, launches per step)."""
+        o = eng.opts(algo=algo, skip_validation=True, stage_timing=stage_timing)
+        rep = _lib.SpgReport()
+        total = 0.0
+        launches = 0
+        stages = {}
+        for _ in range(k):
+            flush.zero_()
+            c = _lib.SpgCsr()
+            barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.multiply_raw(sa, sa, o, c, rep)
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+            launches += rep.kernel_launches
+            for i, nm in enumerate(_lib.STAGES):
+                stages[nm] = stages.get(nm, 0.0) + rep.ms_stage[i]
+            nnz_c = rep.nnz_c
+            eng.free_raw(c)
+        return total / k, rep, launches / k, {s: v / k for s, v in stages.items() if v}, nnz_c
+
+    if args.profile:
+        run_steps(args.profile, args.warmup)
+        ms, rep, _, _, nnz_c = run_steps(args.profile, args.steps)
+        if rank == 0:
+            print(json.dumps({"profile": args.profile, "grid": args.grid, "ms_per_step": round(ms, 4),
+                              "gflops": round(flops / ms / 1e6, 3), "nnz_c": nnz_c}), flush=True)
+        eng.close()
+        return 0
+
+    # warm-up (also loads the predictor)
+    for algo in ("learned", "plain"):
+        run_steps(algo, args.warmup)
+
+    with ClockSampler(local) as clk:
+        barrier()
+        ms_learned, rep_l, launches_l, _, nnz_c = run_steps("learned", args.steps)
+        ms_learned = max_over_ranks(ms_learned)
+        ms_plain, rep_p, launches_p, _, _ = run_steps("plain", args.steps)
+        ms_plain = max_over_ranks(ms_plain)
+    clocks = clk.summary()
+    # per-stage breakdown (separate, untimed-for-headline runs)
+    _, rep_ls, _, stages_l, _ = run_steps("learned", 2, stage_timing=True)
+    _, rep_ps, _, stages_p, _ = run_steps("plain", 2, stage_timing=True)
+
+    # cuSPARSE SpGEMM (ALG3, as the reference's driver) on the same GPU: reported reference point
+    cus = {}
+    try:
+        ms_c, _, _, _, _ = run_steps("cusparse", 2)
+        cus = {"ms": round(ms_c, 3), "gflops": round(flops / ms_c / 1e6, 3), "alg": "ALG3 chunk 0.01"}
+    except Exception as ex:  # reported, not gated
+        cus = {"error": str(ex)[:200]}
+
+    # end to end through the public API: pinned host inputs -> C back in pinned host memory
+    hA = HostCsr(A, index_bits=32, pinned=True)
+    sh = hA.struct()
+    o_e2e = eng.opts(algo="learned", skip_validation=True)
+    h2d = 2 * (hA.nnz * 8 + (A.rows + 1) * 4)
+    host_c = None
+    e2e_ms = []
+    d2h = 0
+    for i in range(2 + args.steps):
+        c = _lib.SpgCsr()
+        rep = _lib.SpgReport()
+        flush.zero_()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.multiply_raw(sh, sh, o_e2e, c, rep)
+        n = int(c.nnz)
+        if host_c is None:
+            host_c = [torch.empty(A.rows + 1, dtype=torch.int32, pin_memory=True),
+                      torch.empty(n, dtype=torch.int32, pin_memory=True),
+                      torch.empty(n, dtype=torch.float32, pin_memory=True)]
+        sizes = [(A.rows + 1) * (c.index_bits // 8), n * 4, n * 4]
+        eng.download_raw(c, host_c[0].data_ptr(), host_c[1].data_ptr(), host_c[2].data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        if i >= 2:
+            e2e_ms.append(e0.elapsed_time(e1))
+        d2h = sum(sizes)
+        eng.free_raw(c)
+    e2e_ms_step = max_over_ranks(statistics.mean(e2e_ms))
+
+    # roofline of the dominant kernel (numeric stage of the learned path)
+    bytes_alg = csr_bytes(A.rows, A.nnz) * 2 + csr_bytes(A.rows, nnz_c)
+    t_num = stages_l.get("numeric", 0.0)
+    peak, peak_kind = load_peaks()
+    achieved = bytes_alg / (t_num * 1e-3) / 1e9 if t_num else None
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
+                "traffic": traffic_from_profiles("k_num_warp_learned"),
+                "kernel": "numeric stage (k_num_warp_learned)", "peak_kind": peak_kind,
+                "algorithmic_bytes": int(bytes_alg), "kernel_ms": round(t_num, 4),
+                "whole_call_frac": round(bytes_alg / (ms_learned * 1e-3) / 1e9 / peak, 4)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, info = cpu_sample(A, args.cpu_seconds)
+        cpu = {"value": round(v, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
+               "sample": f"leading {info['rows']} rows of the same C=A*A ({info['products']} products, "
+                         f"{info['seconds']:.1f} s)"}
+
+    value = world * flops / (ms_learned * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_learned, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rows": A.rows, "nnz_a": A.nnz, "products": products, "nnz_c": nnz_c,
+                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before every step",
+                   "index": "int32 CSR"},
+        "plain": {"ms": round(ms_plain, 4), "gflops": round(world * flops / (ms_plain * 1e-3) / 1e9, 3),
+                  "stages_ms": {k: round(v, 4) for k, v in stages_p.items()}},
+        "learned": {"ms": round(ms_learned, 4), "stages_ms": {k: round(v, 4) for k, v in stages_l.items()},
+                    "rows_predicted": rep_ls.rows_predicted, "rows_overflow": rep_ls.rows_overflow,
+                    "misprediction_rate": round(rep_ls.rows_overflow / max(1, rep_ls.rows_predicted), 6)},
+        "speedup_learned_vs_plain": round(ms_plain / ms_learned, 4),
+        "cusparse": cus,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(world * flops / (e2e_ms_step * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
+                "ms_per_step": round(e2e_ms_step, 4), "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(round(launches_l * args.steps)),
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

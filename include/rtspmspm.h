@@ -172,6 +172,15 @@ spg_status spg_csr_free(spg_ctx* ctx, spg_csr* m);
 /* Copies a matrix to SPG_HOST or SPG_DEVICE (library-owned result). */
 spg_status spg_csr_copy(spg_ctx* ctx, const spg_csr* src, int32_t location, spg_csr* dst);
 
+/*
+ * Copies a device matrix into caller-provided host buffers (rows+1 row
+ * pointers of src->index_bits width, nnz columns, nnz values; pinned memory
+ * gives full PCIe/C2C bandwidth) and waits for the copy.  Replaces the
+ * reference's device-to-host result copies (optixSpMSpM.cpp:462-463,
+ * cuSparse/src/main.cpp:555-558).
+ */
+spg_status spg_csr_download(spg_ctx* ctx, const spg_csr* src, void* row_ptr, int32_t* col_idx, float* val);
+
 /* ---- Matrix Market IO (host) --------------------------------------------- */
 
 /*
@@ -259,7 +268,8 @@ typedef struct spg_tuning {
     int32_t block_table_max;   /* CTA hash table for the symbolic mid bin */
     float   predict_margin;    /* learned: capacity = margin * predicted + slack */
     int32_t predict_slack;
-    int32_t reserved[5];
+    float   learned_load;      /* learned: table load factor at the predicted capacity */
+    int32_t reserved[4];
 } spg_tuning;
 
 spg_status spg_get_tuning(spg_ctx* ctx, spg_tuning* out);

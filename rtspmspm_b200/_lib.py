@@ -85,7 +85,8 @@ class SpgTuning(ctypes.Structure):
     _fields_ = [("warp_table_max", ctypes.c_int32), ("warps_per_block", ctypes.c_int32),
                 ("max_load", ctypes.c_float), ("tile_cols", ctypes.c_int32),
                 ("block_table_max", ctypes.c_int32), ("predict_margin", ctypes.c_float),
-                ("predict_slack", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+                ("predict_slack", ctypes.c_int32), ("learned_load", ctypes.c_float),
+                ("reserved", ctypes.c_int32 * 4)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
@@ -107,6 +108,7 @@ SIGNATURES = [
      [_vp, ctypes.c_int32, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
     ("spg_csr_free", ctypes.c_int32, [_vp, _P(SpgCsr)]),
     ("spg_csr_copy", ctypes.c_int32, [_vp, _P(SpgCsr), ctypes.c_int32, _P(SpgCsr)]),
+    ("spg_csr_download", ctypes.c_int32, [_vp, _P(SpgCsr), _vp, _vp, _vp]),
     ("spg_mtx_read", ctypes.c_int32, [ctypes.c_char_p, _P(SpgCsr)]),
     ("spg_mtx_write", ctypes.c_int32, [_vp, ctypes.c_char_p, _P(SpgCsr), ctypes.c_int32]),
     ("spg_mlp_load", ctypes.c_int32, [_vp, ctypes.c_char_p]),

@@ -68,6 +68,7 @@ spg_tuning default_tuning() {
   t.block_table_max = 16384;
   t.predict_margin = 1.25f;
   t.predict_slack = 8;
+  t.learned_load = 0.7f;
   return t;
 }
 
@@ -423,7 +424,13 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
                       lc);
   ctx->launches += 3;
   tm.mark(SPG_STAGE_BINNING);
-  P.bin(cap.as<int64_t>(), kBinLearned);
+  {
+    BinParams lbp = P.bp;
+    lbp.max_load = std::min(0.9f, std::max(0.1f, P.tune.learned_load > 0.f ? P.tune.learned_load : P.bp.max_load));
+    launch_binning(cap.as<int64_t>(), rows, P.cols, kBinLearned, lbp, P.bin_of_row.as<uint8_t>(), P.counts(),
+                   P.offsets(), P.cursors(), P.lists.as<int32_t>(), lc);
+    ctx->launches += 3;
+  }
   launch_excl_scan(cap.as<int64_t>(), rows, slab_off.as<int64_t>(), P.scan_tmp.as<int64_t>(), lc);
   ctx->launches += 4;
   int64_t slab_total = 0;
@@ -711,6 +718,21 @@ spg_status spg_csr_copy(spg_ctx* ctx, const spg_csr* src, int32_t location, spg_
   }
   SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   *dst = d;
+  return SPG_OK;
+}
+
+spg_status spg_csr_download(spg_ctx* ctx, const spg_csr* src, void* row_ptr, int32_t* col_idx, float* val) {
+  if (!ctx || !src || !row_ptr || (src->nnz > 0 && (!col_idx || !val))) return SPG_ERR_INVALID_ARG;
+  if (src->location != SPG_DEVICE) return fail(ctx, SPG_ERR_INVALID_ARG, "spg_csr_download needs a device matrix");
+  SPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t rpb = (size_t)(src->rows + 1) * (src->index_bits / 8);
+  const size_t nb = (size_t)src->nnz * 4;
+  SPG_CUDA(ctx, cudaMemcpyAsync(row_ptr, src->row_ptr, rpb, cudaMemcpyDeviceToHost, ctx->stream));
+  if (nb) {
+    SPG_CUDA(ctx, cudaMemcpyAsync(col_idx, src->col_idx, nb, cudaMemcpyDeviceToHost, ctx->stream));
+    SPG_CUDA(ctx, cudaMemcpyAsync(val, src->val, nb, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return SPG_OK;
 }
 

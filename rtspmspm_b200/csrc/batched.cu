@@ -136,7 +136,8 @@ __global__ void __launch_bounds__(kBatchWarps * 32) k_batch_rows(const BatchMat*
           int cnt = 0;
           switch (logt) {
 #define SPG_SYM(L) \
-  case L: cnt = symbolic_row<L>(M.A, M.B, r, keys, flags); break;
+  case L: cnt = symbolic_row<L>(M.A, M.B, r, keys, M.B.cols < (1 << 24) ? (int)((i - first) / usable) : -1, flags); \
+    break;
             SPG_SYM(5) SPG_SYM(6) SPG_SYM(7) SPG_SYM(8) SPG_SYM(9) SPG_SYM(10) SPG_SYM(11) SPG_SYM(12)
 #undef SPG_SYM
             default: break;

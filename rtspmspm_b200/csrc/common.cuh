@@ -126,6 +126,29 @@ __device__ __forceinline__ int hash_insert(int32_t* keys, int log_t, int32_t j, 
   return -1;
 }
 
+// Epoch-tagged keys-only table for counting: a slot holds (epoch << 24) | j,
+// and a slot whose epoch differs from the current one counts as empty, so
+// the table needs no clearing between rows (columns must be < 2^24).
+// Returns true when j was new for this epoch.
+__device__ __forceinline__ bool tagged_insert(int32_t* keys, int log_t, int32_t j, uint32_t epoch, int* flags) {
+  const uint32_t mask = (1u << log_t) - 1u;
+  const int32_t want = (int32_t)((epoch << 24) | (uint32_t)j);
+  uint32_t s = hash_slot(j, log_t);
+  for (uint32_t probe = 0; probe <= mask;) {
+    const int32_t k = keys[s];
+    if (k == want) return false;
+    if (((uint32_t)k >> 24) != epoch) {
+      const int32_t old = atomicCAS(&keys[s], k, want);
+      if (old == k) return true;
+      continue;  // the slot changed under us: look at it again
+    }
+    s = (s + 1u) & mask;
+    ++probe;
+  }
+  raise_flag(flags, kFlagHashFull);
+  return false;
+}
+
 // Looks up key j; returns its slot or -1.
 __device__ __forceinline__ int hash_find(const int32_t* keys, int log_t, int32_t j) {
   const uint32_t mask = (1u << log_t) - 1u;

@@ -250,10 +250,18 @@ __global__ void k_sym_warp(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, i
   __syncwarp();
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  // epoch-tagged keys need no per-row clearing (columns < 2^24)
+  const bool tagged = B.cols < (1 << 24);
+  int epoch = tagged ? 0 : -1;
   for (int64_t idx = gw; idx < nrows; idx += nw) {
     const int32_t row = rows[idx];
-    const int cnt = symbolic_row<LOGT>(A, B, row, keys, flags);
+    const int cnt = symbolic_row<LOGT>(A, B, row, keys, epoch, flags);
     if (lane == 0) nnz_out[row] = cnt;
+    if (tagged && ++epoch == 255) {
+      for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
+      __syncwarp();
+      epoch = 0;
+    }
   }
 }
 

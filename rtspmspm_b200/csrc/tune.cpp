@@ -129,6 +129,7 @@ spg_status spg_set_tuning(spg_ctx* ctx, const spg_tuning* in) {
   if (t.tile_cols == 0) t.tile_cols = d.tile_cols;
   if (t.predict_margin <= 0.f) t.predict_margin = d.predict_margin;
   if (t.predict_slack < 0) t.predict_slack = d.predict_slack;
+  if (!(t.learned_load > 0.05f && t.learned_load < 0.95f)) t.learned_load = d.learned_load;
   ctx->tuning = t;
   return SPG_OK;
 }
@@ -163,6 +164,7 @@ spg_status spg_tune(spg_ctx* ctx, int32_t n, const spg_csr* A, const spg_csr* B,
           t.block_table_max = bt;
           t.predict_margin = saved.predict_margin;
           t.predict_slack = saved.predict_slack;
+          t.learned_load = saved.learned_load;
           ctx->tuning = t;
           spg_opts o{};
           o.algo = SPG_ALGO_PLAIN;

@@ -7,14 +7,30 @@
 
 namespace spg {
 
+// Prefetch depth: B-row steps whose first 32 entries are loaded before any
+// of them is inserted, so a warp keeps kPrefetch independent loads in flight
+// instead of one dependent load per step.
+constexpr int kPrefetch = 8;
+
 // Exact number of distinct output columns of `row` (keys-only table).
-// Leaves the table cleared.
+// epoch >= 0: epoch-tagged table (no clearing; caller advances the epoch and
+// clears the table when it wraps).  epoch < 0: plain keys, cleared here.
 template <int LOGT>
-__device__ __forceinline__ int symbolic_row(const DCsr& A, const DCsr& B, int32_t row, int32_t* keys, int* flags) {
+__device__ __forceinline__ int symbolic_row(const DCsr& A, const DCsr& B, int32_t row, int32_t* keys, int epoch,
+                                            int* flags) {
   constexpr int T = 1 << LOGT;
   const int lane = lane_id();
   const int64_t s = A.rp[row], e = A.rp[row + 1];
   int cnt = 0;
+  auto insert = [&](int32_t j) {
+    if (epoch >= 0) {
+      cnt += tagged_insert(keys, LOGT, j, (uint32_t)epoch, flags);
+    } else {
+      bool fresh;
+      hash_insert(keys, LOGT, j, fresh, flags);
+      cnt += fresh;
+    }
+  };
   for (int64_t base = s; base < e; base += 32) {
     const int64_t p = base + lane;
     int64_t bs = 0, be = 0;
@@ -24,26 +40,40 @@ __device__ __forceinline__ int symbolic_row(const DCsr& A, const DCsr& B, int32_
       be = B.rp[k + 1];
     }
     const int n = (int)min((int64_t)32, e - base);
-    for (int t = 0; t < n; ++t) {
-      const int64_t bst = __shfl_sync(kFull, bs, t), ben = __shfl_sync(kFull, be, t);
-      for (int64_t q = bst + lane; q < ben; q += 32) {
-        bool fresh;
-        hash_insert(keys, LOGT, B.col[q], fresh, flags);
-        cnt += fresh;
+    for (int t0 = 0; t0 < n; t0 += 2 * kPrefetch) {
+      int32_t c[2 * kPrefetch];
+#pragma unroll
+      for (int d = 0; d < 2 * kPrefetch; ++d) {
+        const int t = t0 + d;
+        const int64_t bst = __shfl_sync(kFull, bs, t & 31), ben = __shfl_sync(kFull, be, t & 31);
+        const int64_t q = bst + lane;
+        c[d] = (t < n && q < ben) ? B.col[q] : -1;
+      }
+#pragma unroll
+      for (int d = 0; d < 2 * kPrefetch; ++d)
+        if (c[d] >= 0) insert(c[d]);
+      // entries beyond the first 32 of long B rows (symbolic order is free)
+      for (int d = 0; d < 2 * kPrefetch && t0 + d < n; ++d) {
+        const int t = t0 + d;
+        const int64_t bst = __shfl_sync(kFull, bs, t), ben = __shfl_sync(kFull, be, t);
+        for (int64_t q = bst + 32 + lane; q < ben; q += 32) insert(B.col[q]);
       }
     }
   }
   __syncwarp();
   cnt = warp_sum(cnt);
-  for (int s2 = lane; s2 < T; s2 += 32) keys[s2] = kEmpty;
-  __syncwarp();
+  if (epoch < 0) {
+    for (int s2 = lane; s2 < T; s2 += 32) keys[s2] = kEmpty;
+    __syncwarp();
+  }
   return cnt;
 }
 
 // Accumulates row `row` into the warp's table in canonical order: k-serial
 // (one B row at a time), lanes parallel over the columns of B_k.  Within
 // one B row all columns are distinct, so each slot receives at most one
-// product per step; __syncwarp orders the steps.
+// product per step; __syncwarp orders the steps.  The first 32 entries of
+// kPrefetch consecutive B rows are loaded before the group is inserted.
 // With cap >= 0 the row aborts (returns false) as soon as more than `cap`
 // distinct columns appear or the table fills: the learned path's overflow.
 template <int LOGT>
@@ -63,27 +93,52 @@ __device__ __forceinline__ bool accumulate_row(const DCsr& A, const DCsr& B, int
       be = B.rp[k + 1];
     }
     const int n = (int)min((int64_t)32, e - base);
-    for (int t = 0; t < n; ++t) {
-      const int64_t bst = __shfl_sync(kFull, bs, t), ben = __shfl_sync(kFull, be, t);
-      const float at = __shfl_sync(kFull, a, t);
-      for (int64_t q0 = bst; q0 < ben; q0 += 32) {
-        const int64_t q = q0 + lane;
-        bool fresh = false, failed = false;
-        if (q < ben) {
-          const int32_t j = B.col[q];
-          const float pr = prod_rn(at, B.val[q]);
-          const int slot = hash_insert(keys, LOGT, j, fresh, cap >= 0 ? nullptr : flags);
-          if (slot >= 0) vals[slot] = add_rn(vals[slot], pr);
-          else failed = true;
-        }
-        count += __popc(__ballot_sync(kFull, fresh));
-        if (cap >= 0 && (__any_sync(kFull, failed) || count > cap)) {
-          __syncwarp();
-          distinct = count;
-          return false;
-        }
+    for (int t0 = 0; t0 < n; t0 += kPrefetch) {
+      int32_t c[kPrefetch];
+      float v[kPrefetch];
+#pragma unroll
+      for (int d = 0; d < kPrefetch; ++d) {
+        const int t = t0 + d;
+        const int64_t bst = __shfl_sync(kFull, bs, t & 31), ben = __shfl_sync(kFull, be, t & 31);
+        const int64_t q = bst + lane;
+        const bool ok = t < n && q < ben;
+        c[d] = ok ? B.col[q] : -1;
+        v[d] = ok ? B.val[q] : 0.f;
       }
-      __syncwarp();
+#pragma unroll
+      for (int d = 0; d < kPrefetch; ++d) {
+        const int t = t0 + d;
+        if (t >= n) break;  // warp-uniform
+        const float at = __shfl_sync(kFull, a, t);
+        const int64_t bst = __shfl_sync(kFull, bs, t), ben = __shfl_sync(kFull, be, t);
+        // first chunk (prefetched), then the rest of B_k, all before B_{k+1}
+        for (int64_t q0 = bst; q0 < ben; q0 += 32) {
+          const int64_t q = q0 + lane;
+          int32_t j = -1;
+          float bv = 0.f;
+          if (q0 == bst) {
+            j = c[d];
+            bv = v[d];
+          } else if (q < ben) {
+            j = B.col[q];
+            bv = B.val[q];
+          }
+          bool fresh = false, failed = false;
+          if (j >= 0) {
+            const float pr = prod_rn(at, bv);
+            const int slot = hash_insert(keys, LOGT, j, fresh, cap >= 0 ? nullptr : flags);
+            if (slot >= 0) vals[slot] = add_rn(vals[slot], pr);
+            else failed = true;
+          }
+          count += __popc(__ballot_sync(kFull, fresh));
+          if (cap >= 0 && (__any_sync(kFull, failed) || count > cap)) {
+            __syncwarp();
+            distinct = count;
+            return false;
+          }
+        }
+        __syncwarp();
+      }
     }
   }
   distinct = count;

@@ -224,6 +224,10 @@ class Engine:
         self._check(self.L.spg_multiply(self.ctx, ctypes.byref(sa), ctypes.byref(sb), ctypes.byref(c),
                                         ctypes.byref(o), ctypes.byref(rep)))
 
+    def download_raw(self, c: _lib.SpgCsr, row_ptr: int, col_idx: int, val: int) -> None:
+        """Copies a device C into caller host buffers (raw pointers) and waits."""
+        self._check(self.L.spg_csr_download(self.ctx, ctypes.byref(c), row_ptr, col_idx, val))
+
     def free_raw(self, c: _lib.SpgCsr) -> None:
         self.L.spg_csr_free(self.ctx, ctypes.byref(c))
 

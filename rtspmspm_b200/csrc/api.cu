@@ -63,12 +63,12 @@ spg_tuning default_tuning() {
   spg_tuning t{};
   t.warp_table_max = 4096;
   t.warps_per_block = 8;
-  t.max_load = 0.5f;
+  t.max_load = 0.3f;
   t.tile_cols = kTileCols;
   t.block_table_max = 16384;
   t.predict_margin = 1.25f;
   t.predict_slack = 8;
-  t.learned_load = 0.7f;
+  t.learned_load = 0.4f;
   return t;
 }
 
@@ -83,7 +83,8 @@ BinParams bin_params(const spg_tuning& t) {
   int lg = ilog2_floor(std::max(32, std::min(4096, t.warp_table_max)));
   bp.warp_log_max = std::max(kMinLogT, std::min(kMaxLogT, lg));
   bp.max_load = std::min(0.9f, std::max(0.1f, t.max_load));
-  bp.warp_cap = (int64_t)std::floor((double)(1 << bp.warp_log_max) * bp.max_load);
+  // the largest table may run up to half full whatever the load factor
+  bp.warp_cap = (int64_t)std::floor((double)(1 << bp.warp_log_max) * std::max(0.5f, bp.max_load));
   // symbolic CTA table at load <= 2/3
   int blg = ilog2_floor(std::max(1024, std::min(32768, t.block_table_max)));
   bp.block_cap = ((int64_t)1 << blg) * 2 / 3;
@@ -136,15 +137,23 @@ spg_status prepare_matrix(spg_ctx* ctx, const spg_csr* m, DevMat& out, bool vali
     return fail(ctx, SPG_ERR_INVALID_ARG, "location must be SPG_HOST or SPG_DEVICE");
   }
   const int64_t* rp64;
+  const int32_t* rp32 = nullptr;
   if (m->index_bits == 32) {
     SPG_TRY(out.rp64.alloc(ctx, (size_t)(m->rows + 1) * 8));
     launch_widen_rp(static_cast<const int32_t*>(rp), m->rows + 1, out.rp64.as<int64_t>(), lc);
     ++ctx->launches;
     rp64 = out.rp64.as<int64_t>();
+    rp32 = static_cast<const int32_t*>(rp);
   } else {
     rp64 = static_cast<const int64_t*>(rp);
+    if (m->nnz < INT32_MAX) {
+      SPG_TRY(out.rp32.alloc(ctx, (size_t)(m->rows + 1) * 4));
+      launch_narrow_rp(rp64, m->rows + 1, out.rp32.as<int32_t>(), lc);
+      ++ctx->launches;
+      rp32 = out.rp32.as<int32_t>();
+    }
   }
-  out.view = DCsr{m->rows, m->cols, rp64, col, val};
+  out.view = DCsr{m->rows, m->cols, rp64, col, val, rp32};
   out.nnz = m->nnz;
   if (validate) {
     launch_validate(out.view, m->nnz, ctx->d_flags, lc);
@@ -408,21 +417,18 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
   const LaunchCtx lc = P.lc;
   SPG_TRY(ensure_mlp(ctx));
   const int64_t rows = P.rows;
-  DevBuf feats, cap, need, slab_off, key;
-  SPG_TRY(feats.alloc(ctx, (size_t)std::max<int64_t>(rows, 1) * kMlpIn * 4));
+  DevBuf cap, need, slab_off, key;
   SPG_TRY(cap.alloc(ctx, (size_t)(rows + 1) * 8));
   SPG_TRY(need.alloc(ctx, (size_t)std::max<int64_t>(rows, 1)));
   SPG_TRY(slab_off.alloc(ctx, (size_t)(rows + 1) * 8));
   SPG_TRY(key.alloc(ctx, (size_t)std::max<int64_t>(rows, 1) * 8));
-  tm.mark(SPG_STAGE_FEATURES);
-  launch_features(P.A.view, P.B.view, feats.as<float>(), P.prod.as<int64_t>(), lc);
+  // products, features and the tensor-core MLP in one pass over A
+  tm.mark(SPG_STAGE_MLP);
+  launch_learned_plan(P.A.view, P.B.view, ctx->mlp_w16, P.tune.predict_margin, P.tune.predict_slack, P.bp.warp_cap,
+                      o.force_overflow, P.prod.as<int64_t>(), cap.as<int64_t>(), need.as<uint8_t>(), lc);
   SPG_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, 4 * 8, ctx->stream));
   launch_sum(P.prod.as<int64_t>(), rows, ctx->d_counter + 1, lc);
-  tm.mark(SPG_STAGE_MLP);
-  launch_mlp_capacity(ctx->mlp_w16, feats.as<float>(), P.prod.as<int64_t>(), rows, P.cols, P.tune.predict_margin,
-                      P.tune.predict_slack, P.bp.warp_cap, o.force_overflow, cap.as<int64_t>(), need.as<uint8_t>(),
-                      lc);
-  ctx->launches += 3;
+  ctx->launches += 2;
   tm.mark(SPG_STAGE_BINNING);
   {
     BinParams lbp = P.bp;

@@ -77,7 +77,7 @@ __global__ void k_batch_bound_stats(const int32_t* row_mat, const int64_t* bound
 }
 
 __device__ __forceinline__ int warps_usable(int logt, bool numeric) {
-  const int per_warp = (1 << logt) * (numeric ? 8 : 4);
+  const int per_warp = (1 << logt) * (numeric ? 12 : 4);
   int w = kBatchArenaBytes / per_warp;
   return w < 1 ? 1 : (w > kBatchWarps ? kBatchWarps : w);
 }
@@ -121,22 +121,24 @@ __global__ void __launch_bounds__(kBatchWarps * 32) k_batch_rows(const BatchMat*
     const int64_t last = min(first + per, bin_off[bin + 1]);
     if (w < usable) {
       const int T = 1 << logt;
-      int32_t* keys = arena + (size_t)w * T * (NUMERIC ? 2 : 1);
+      int32_t* keys = arena + (size_t)w * T * (NUMERIC ? 3 : 1);
       float* vals = reinterpret_cast<float*>(keys + T);
-      for (int s = lane; s < T; s += 32) {
-        keys[s] = kEmpty;
-        if (NUMERIC) vals[s] = 0.f;
-      }
+      int32_t* list = keys + 2 * T;
+      for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
       __syncwarp();
+      int epoch = 0;  // at most kRowsPerWarpTile rows per tile: no wrap
       for (int64_t i = first + w; i < last; i += usable) {
         const int64_t g = lists[i];
         const BatchMat& M = mats[row_mat[g]];
         const int32_t r = (int32_t)(g - M.row_start);
+        const int ep = M.B.cols < (1 << 24) ? epoch : kNoEpoch;
         if (!NUMERIC) {
           int cnt = 0;
           switch (logt) {
-#define SPG_SYM(L) \
-  case L: cnt = symbolic_row<L>(M.A, M.B, r, keys, M.B.cols < (1 << 24) ? (int)((i - first) / usable) : -1, flags); \
+#define SPG_SYM(L)                                                                                    \
+  case L:                                                                                             \
+    cnt = M.B.rp32 ? symbolic_row<L, true>(M.A, M.B, r, keys, ep, flags)                              \
+                   : symbolic_row<L, false>(M.A, M.B, r, keys, ep, flags);                            \
     break;
             SPG_SYM(5) SPG_SYM(6) SPG_SYM(7) SPG_SYM(8) SPG_SYM(9) SPG_SYM(10) SPG_SYM(11) SPG_SYM(12)
 #undef SPG_SYM
@@ -147,14 +149,19 @@ __global__ void __launch_bounds__(kBatchWarps * 32) k_batch_rows(const BatchMat*
           const int64_t base = gscan[M.row_start];
           const int64_t off = M.c_base + (gscan[g] - base);
           const int64_t want = gscan[g + 1] - gscan[g];
+          int e2 = ep;
           switch (logt) {
-#define SPG_NUM(L) \
-  case L: numeric_row<L>(M.A, M.B, r, keys, vals, c_col + off, c_val + off, want, flags); break;
+#define SPG_NUM(L)                                                                                      \
+  case L:                                                                                               \
+    if (M.B.rp32) numeric_row<L, true>(M.A, M.B, r, keys, vals, list, e2, c_col + off, c_val + off, want, flags); \
+    else numeric_row<L, false>(M.A, M.B, r, keys, vals, list, e2, c_col + off, c_val + off, want, flags);         \
+    break;
             SPG_NUM(5) SPG_NUM(6) SPG_NUM(7) SPG_NUM(8) SPG_NUM(9) SPG_NUM(10) SPG_NUM(11) SPG_NUM(12)
 #undef SPG_NUM
             default: break;
           }
         }
+        ++epoch;
       }
     }
     __syncthreads();
@@ -319,15 +326,23 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
     for (int q = 0; q < 2; ++q) {
       const spg_csr* x = src[q];
       const int64_t* rp64;
+      const int32_t* rp32 = nullptr;
       if (x->index_bits == 32) {
         int64_t* w = nullptr;
         SPG_TRY(dmalloc(ctx, p, &w, (size_t)x->rows + 1));
         launch_widen_rp(static_cast<const int32_t*>(x->row_ptr), x->rows + 1, w, lc);
         rp64 = w;
+        rp32 = static_cast<const int32_t*>(x->row_ptr);
       } else {
         rp64 = static_cast<const int64_t*>(x->row_ptr);
+        if (x->nnz < INT32_MAX) {
+          int32_t* w = nullptr;
+          SPG_TRY(dmalloc(ctx, p, &w, (size_t)x->rows + 1));
+          launch_narrow_rp(rp64, x->rows + 1, w, lc);
+          rp32 = w;
+        }
       }
-      *dst[q] = DCsr{x->rows, x->cols, rp64, x->col_idx, x->val};
+      *dst[q] = DCsr{x->rows, x->cols, rp64, x->col_idx, x->val, rp32};
       if (!o.skip_validation) launch_validate(*dst[q], x->nnz, ctx->d_flags, lc);
     }
     M.row_start = R;

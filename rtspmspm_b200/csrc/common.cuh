@@ -26,13 +26,28 @@ constexpr int kFlagWaitLimit = 2;
 constexpr int kFlagBadIndex = 4;
 constexpr int kFlagCountDiff = 8;
 
-// Read-only device view of a CSR matrix with 64-bit row pointers.
+// Read-only device view of a CSR matrix.  `rp` always holds 64-bit row
+// pointers; `rp32` holds the same offsets as int32 when nnz < 2^31 (else
+// null), so the hot loops can move half the bytes and shuffle one register.
 struct DCsr {
   int64_t rows;
   int64_t cols;
   const int64_t* rp;
   const int32_t* col;
   const float* val;
+  const int32_t* rp32;
+};
+
+// Row offset type of the hot loops: int32 when R32, else int64.
+template <bool R32>
+struct RowOff {
+  using T = int64_t;
+  static __device__ __forceinline__ int64_t at(const DCsr& M, int64_t i) { return M.rp[i]; }
+};
+template <>
+struct RowOff<true> {
+  using T = int32_t;
+  static __device__ __forceinline__ int32_t at(const DCsr& M, int64_t i) { return M.rp32[i]; }
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -162,39 +177,44 @@ __device__ __forceinline__ int hash_find(const int32_t* keys, int log_t, int32_t
   return -1;
 }
 
-// Sorts n (key, value) pairs held in shared memory by key, using one warp
-// (bitonic network over next_pow2(n) <= cap slots; slots [n, np2) are filled
-// with +inf keys first).  Keys are distinct column indices.
-__device__ __forceinline__ void warp_sort_pairs(int32_t* keys, float* vals, int n, int cap) {
+// Bitonic sort of 32*E keys held in registers, E per lane; element index =
+// lane * E + e, ascending after the call.
+template <int E>
+__device__ __forceinline__ void warp_sort_keys_regs(int32_t (&key)[E]) {
   const int lane = lane_id();
-  int np2 = 1;
-  while (np2 < n) np2 <<= 1;
-  if (np2 > cap) np2 = cap;  // caller guarantees np2 <= cap
-  for (int s = n + lane; s < np2; s += 32) keys[s] = 0x7fffffff;
-  __syncwarp();
-  for (int size = 2; size <= np2; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int i = lane; i < (np2 >> 1); i += 32) {
-        // i-th compare pair: lo index has bit `stride` clear
-        int lo = ((i & ~(stride - 1)) << 1) | (i & (stride - 1));
-        int hi = lo | stride;
-        bool up = (lo & size) == 0;
-        int32_t a = keys[lo], b = keys[hi];
-        if ((a > b) == up) {
-          keys[lo] = b;
-          keys[hi] = a;
-          float va = vals[lo], vb = vals[hi];
-          vals[lo] = vb;
-          vals[hi] = va;
+  constexpr int N = 32 * E;
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int s = k >> 1; s > 0; s >>= 1) {
+      if (s >= E) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int idx = lane * E + e;
+          const int32_t pk = __shfl_xor_sync(kFull, key[e], s / E);
+          const bool keep_small = ((idx & s) == 0) == ((idx & k) == 0);
+          key[e] = keep_small ? min(pk, key[e]) : max(pk, key[e]);
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int f = e ^ s;
+          if (f > e) {
+            const int idx = lane * E + e;
+            const bool asc = (idx & k) == 0;
+            const int32_t x = key[e], y = key[f];
+            key[e] = asc ? min(x, y) : max(x, y);
+            key[f] = asc ? max(x, y) : min(x, y);
+          }
         }
       }
-      __syncwarp();
     }
   }
 }
 
-// Key-only variant of warp_sort_pairs.
-__device__ __forceinline__ void warp_sort_keys(int32_t* keys, int n, int cap) {
+// Sorts n distinct keys held in shared memory with one warp (bitonic network
+// over next_pow2(n) <= cap slots; slots [n, np2) are padded with +inf).
+static __device__ __noinline__ void warp_sort_keys(int32_t* keys, int n, int cap) {
   const int lane = lane_id();
   int np2 = 1;
   while (np2 < n) np2 <<= 1;

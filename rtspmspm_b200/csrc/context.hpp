@@ -90,6 +90,7 @@ struct DevMat {
   DCsr view{};
   int64_t nnz = 0;
   DevBuf rp64;      // widened row pointers when the input had int32 ones
+  DevBuf rp32;      // narrowed row pointers when the input had int64 ones and nnz < 2^31
   DevBuf upload[3]; // copies of host inputs
 };
 

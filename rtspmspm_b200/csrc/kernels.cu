@@ -240,8 +240,8 @@ __global__ void k_store_total(const int64_t* excl_last, const int64_t* in_last, 
 // --------------------------------------------------------------------------
 
 // Warp per row; per-warp key table of 2^LOGT slots in shared memory.
-template <int LOGT>
-__global__ void k_sym_warp(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, int64_t* nnz_out, int* flags) {
+template <int LOGT, bool R32>
+__global__ void __launch_bounds__(512, 2) k_sym_warp(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, int64_t* nnz_out, int* flags) {
   constexpr int T = 1 << LOGT;
   extern __shared__ int32_t sm_keys[];
   const int lane = lane_id();
@@ -251,17 +251,12 @@ __global__ void k_sym_warp(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, i
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   // epoch-tagged keys need no per-row clearing (columns < 2^24)
-  const bool tagged = B.cols < (1 << 24);
-  int epoch = tagged ? 0 : -1;
+  int epoch = B.cols < (1 << 24) ? 0 : kNoEpoch;
   for (int64_t idx = gw; idx < nrows; idx += nw) {
     const int32_t row = rows[idx];
-    const int cnt = symbolic_row<LOGT>(A, B, row, keys, epoch, flags);
+    const int cnt = symbolic_row<LOGT, R32>(A, B, row, keys, epoch, flags);
     if (lane == 0) nnz_out[row] = cnt;
-    if (tagged && ++epoch == 255) {
-      for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
-      __syncwarp();
-      epoch = 0;
-    }
+    if (epoch >= 0) next_row<LOGT>(keys, epoch);
   }
 }
 
@@ -394,76 +389,64 @@ __global__ void k_sym_dense(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, 
 // --------------------------------------------------------------------------
 
 // Plain numeric pass: exact nnz known, writes straight into C.
-template <int LOGT>
-__global__ void k_num_warp(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, const int64_t* c_rp, int32_t* c_col,
-                           float* c_val, int* flags) {
+template <int LOGT, bool R32>
+__global__ void __launch_bounds__(512, 2) k_num_warp(DCsr A, DCsr B, const int32_t* rows, int64_t nrows,
+                                                     const int64_t* c_rp, int32_t* c_col, float* c_val, int* flags) {
   constexpr int T = 1 << LOGT;
   extern __shared__ int32_t sm_tab[];
   const int lane = lane_id();
-  int32_t* keys = sm_tab + (threadIdx.x >> 5) * (2 * T);
+  int32_t* keys = sm_tab + (threadIdx.x >> 5) * numeric_words<LOGT>();
   float* vals = reinterpret_cast<float*>(keys + T);
-  for (int s = lane; s < T; s += 32) {
-    keys[s] = kEmpty;
-    vals[s] = 0.f;
-  }
+  int32_t* list = keys + 2 * T;
+  for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
   __syncwarp();
+  int epoch = B.cols < (1 << 24) ? 0 : kNoEpoch;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t idx = gw; idx < nrows; idx += nw) {
     const int32_t row = rows[idx];
     const int64_t off = c_rp[row];
-    numeric_row<LOGT>(A, B, row, keys, vals, c_col + off, c_val + off, c_rp[row + 1] - off, flags);
+    numeric_row<LOGT, R32>(A, B, row, keys, vals, list, epoch, c_col + off, c_val + off, c_rp[row + 1] - off, flags);
   }
 }
 
 // Learned single-pass numeric: table sized by the predicted capacity; the
 // row is written sorted into its slab slot.  Rows whose distinct count
 // exceeds their capacity are queued for the exact re-run (nnz_out = -1).
-template <int LOGT>
-__global__ void k_num_warp_learned(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, const int64_t* cap,
-                                   const int64_t* slab_off, int32_t* slab_col, float* slab_val, int64_t* nnz_out,
-                                   int32_t* retry_rows, unsigned long long* retry_count, int* flags) {
+template <int LOGT, bool R32>
+__global__ void __launch_bounds__(512, 2) k_num_warp_learned(DCsr A, DCsr B, const int32_t* rows, int64_t nrows,
+                                                             const int64_t* cap, const int64_t* slab_off,
+                                                             int32_t* slab_col, float* slab_val, int64_t* nnz_out,
+                                                             int32_t* retry_rows, unsigned long long* retry_count,
+                                                             int* flags) {
   constexpr int T = 1 << LOGT;
   extern __shared__ int32_t sm_tab[];
   const int lane = lane_id();
-  int32_t* keys = sm_tab + (threadIdx.x >> 5) * (2 * T);
+  int32_t* keys = sm_tab + (threadIdx.x >> 5) * numeric_words<LOGT>();
   float* vals = reinterpret_cast<float*>(keys + T);
-  for (int s = lane; s < T; s += 32) {
-    keys[s] = kEmpty;
-    vals[s] = 0.f;
-  }
+  int32_t* list = keys + 2 * T;
+  for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
   __syncwarp();
+  int epoch = B.cols < (1 << 24) ? 0 : kNoEpoch;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t idx = gw; idx < nrows; idx += nw) {
     const int32_t row = rows[idx];
-    const int64_t c = cap[row];
-    int distinct;
-    const bool ok = accumulate_row<LOGT>(A, B, row, keys, vals, c, flags, distinct);
-    if (!ok) {
-      // overflow: clear the whole table and queue the row for the exact path
-      for (int s = lane; s < T; s += 32) {
-        keys[s] = kEmpty;
-        vals[s] = 0.f;
-      }
+    const int c = (int)cap[row];
+    const int n = accumulate_row<LOGT, R32, true>(A, B, row, keys, vals, list, epoch, c, flags);
+    if (n < 0) {
+      // overflow: queue the row for the exact path
       if (lane == 0) {
         nnz_out[row] = -1;
-        unsigned long long pos = atomicAdd(retry_count, 1ull);
+        const unsigned long long pos = atomicAdd(retry_count, 1ull);
         retry_rows[pos] = row;
       }
-      __syncwarp();
-      continue;
+    } else {
+      const int64_t off = slab_off[row];
+      emit_row<LOGT>(keys, vals, list, n, epoch, n, slab_col + off, slab_val + off);
+      if (lane == 0) nnz_out[row] = n;
     }
-    const int n = compact_table<LOGT>(keys, vals);
-    warp_sort_pairs(keys, vals, n, T);
-    const int64_t off = slab_off[row];
-    for (int t = lane; t < n; t += 32) {
-      slab_col[off + t] = keys[t];
-      slab_val[off + t] = vals[t];
-    }
-    if (lane == 0) nnz_out[row] = n;
-    __syncwarp();
-    reset_front<LOGT>(keys, vals, n);
+    next_row<LOGT>(keys, epoch);
   }
 }
 
@@ -736,36 +719,32 @@ void launch_excl_scan(const int64_t* in, int64_t n, int64_t* out, int64_t* tmp, 
   k_store_total<<<1, 32, 0, lc.stream>>>(out + n - 1, last, out + n);
 }
 
-template <int LOGT>
+template <int LOGT, bool R32>
 static void sym_warp_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int64_t* nnz, int* flags,
                          const LaunchCtx& lc, int wpb) {
   const size_t smem = (size_t)wpb * (1 << LOGT) * sizeof(int32_t);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_sym_warp<LOGT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  cudaFuncSetAttribute(k_sym_warp<LOGT, R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sym_warp<LOGT>, wpb * 32, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sym_warp<LOGT, R32>, wpb * 32, smem);
   if (per_sm < 1) per_sm = 1;
   const int blocks = grid_for(nrows, wpb, 1, lc.sms * per_sm);
-  k_sym_warp<LOGT><<<blocks, wpb * 32, smem, lc.stream>>>(A, B, rows, nrows, nnz, flags);
+  k_sym_warp<LOGT, R32><<<blocks, wpb * 32, smem, lc.stream>>>(A, B, rows, nrows, nnz, flags);
 }
 
 void launch_sym_warp(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int64_t* nnz,
                      int* flags, const LaunchCtx& lc, int wpb) {
   if (nrows == 0) return;
+  const int w = log_t >= 11 ? std::min(wpb, 8) : wpb;
+#define SPG_SW(L)                                                                   \
+  case L:                                                                           \
+    if (B.rp32) sym_warp_one<L, true>(A, B, rows, nrows, nnz, flags, lc, w);        \
+    else sym_warp_one<L, false>(A, B, rows, nrows, nnz, flags, lc, w);              \
+    break;
   switch (log_t) {
-    case 5: sym_warp_one<5>(A, B, rows, nrows, nnz, flags, lc, wpb); break;
-    case 6: sym_warp_one<6>(A, B, rows, nrows, nnz, flags, lc, wpb); break;
-    case 7: sym_warp_one<7>(A, B, rows, nrows, nnz, flags, lc, wpb); break;
-    case 8: sym_warp_one<8>(A, B, rows, nrows, nnz, flags, lc, wpb); break;
-    case 9: sym_warp_one<9>(A, B, rows, nrows, nnz, flags, lc, wpb); break;
-    case 10: sym_warp_one<10>(A, B, rows, nrows, nnz, flags, lc, wpb); break;
-    case 11: sym_warp_one<11>(A, B, rows, nrows, nnz, flags, lc, std::min(wpb, 8)); break;
-    case 12: sym_warp_one<12>(A, B, rows, nrows, nnz, flags, lc, std::min(wpb, 8)); break;
+    SPG_SW(5) SPG_SW(6) SPG_SW(7) SPG_SW(8) SPG_SW(9) SPG_SW(10) SPG_SW(11) SPG_SW(12)
     default: break;
   }
+#undef SPG_SW
 }
 
 void launch_sym_block(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int log_table,
@@ -773,11 +752,7 @@ void launch_sym_block(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t
                       const LaunchCtx& lc) {
   if (nrows == 0) return;
   const size_t smem = ((size_t)1 << log_table) * sizeof(int32_t);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_sym_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  cudaFuncSetAttribute(k_sym_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sym_block, 512, smem);
   if (per_sm < 1) per_sm = 1;
@@ -792,36 +767,28 @@ void launch_sym_dense(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t
   if (nrows == 0) return;
   const int max_words = kDenseWindowWords;
   const size_t smem = (size_t)max_words * sizeof(uint32_t);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_sym_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  cudaFuncSetAttribute(k_sym_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int blocks = (int)std::min<int64_t>(nrows, (int64_t)lc.sms);
   k_sym_dense<<<blocks, 1024, smem, lc.stream>>>(A, B, rows, nrows, max_words, slot_base, nnz, big_slot, tile_cnt,
                                                  ntiles, flags);
 }
 
-template <int LOGT>
+template <int LOGT, bool R32>
 static void num_warp_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, const int64_t* c_rp,
                          int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb) {
-  const size_t smem = (size_t)wpb * (1 << LOGT) * 8;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_num_warp<LOGT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  const size_t smem = (size_t)wpb * numeric_words<LOGT>() * 4;
+  cudaFuncSetAttribute(k_num_warp<LOGT, R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_warp<LOGT>, wpb * 32, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_warp<LOGT, R32>, wpb * 32, smem);
   if (per_sm < 1) per_sm = 1;
   const int blocks = grid_for(nrows, wpb, 1, lc.sms * per_sm);
-  k_num_warp<LOGT><<<blocks, wpb * 32, smem, lc.stream>>>(A, B, rows, nrows, c_rp, c_col, c_val, flags);
+  k_num_warp<LOGT, R32><<<blocks, wpb * 32, smem, lc.stream>>>(A, B, rows, nrows, c_rp, c_col, c_val, flags);
 }
 
 static int wpb_for(int log_t, int wpb) {
-  // keep a CTA's tables within 64 KB
-  const int per_warp = (1 << log_t) * 8;
-  int lim = (64 * 1024) / per_warp;
+  // keep a CTA's tables within 96 KB
+  const int per_warp = (1 << log_t) * 12;
+  int lim = (96 * 1024) / per_warp;
   if (lim < 1) lim = 1;
   return std::max(1, std::min(wpb, lim));
 }
@@ -830,36 +797,32 @@ void launch_num_warp(int log_t, const DCsr& A, const DCsr& B, const int32_t* row
                      const int64_t* c_rp, int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb) {
   if (nrows == 0) return;
   const int w = wpb_for(log_t, wpb);
+#define SPG_NW(L)                                                                          \
+  case L:                                                                                  \
+    if (B.rp32) num_warp_one<L, true>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); \
+    else num_warp_one<L, false>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w);       \
+    break;
   switch (log_t) {
-    case 5: num_warp_one<5>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); break;
-    case 6: num_warp_one<6>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); break;
-    case 7: num_warp_one<7>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); break;
-    case 8: num_warp_one<8>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); break;
-    case 9: num_warp_one<9>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); break;
-    case 10: num_warp_one<10>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); break;
-    case 11: num_warp_one<11>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); break;
-    case 12: num_warp_one<12>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); break;
+    SPG_NW(5) SPG_NW(6) SPG_NW(7) SPG_NW(8) SPG_NW(9) SPG_NW(10) SPG_NW(11) SPG_NW(12)
     default: break;
   }
+#undef SPG_NW
 }
 
-template <int LOGT>
+template <int LOGT, bool R32>
 static void num_warp_learned_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
                                  const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
                                  int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
                                  const LaunchCtx& lc, int wpb) {
-  const size_t smem = (size_t)wpb * (1 << LOGT) * 8;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_num_warp_learned<LOGT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  const size_t smem = (size_t)wpb * numeric_words<LOGT>() * 4;
+  cudaFuncSetAttribute(k_num_warp_learned<LOGT, R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_warp_learned<LOGT>, wpb * 32, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_warp_learned<LOGT, R32>, wpb * 32, smem);
   if (per_sm < 1) per_sm = 1;
   const int blocks = grid_for(nrows, wpb, 1, lc.sms * per_sm);
-  k_num_warp_learned<LOGT><<<blocks, wpb * 32, smem, lc.stream>>>(A, B, rows, nrows, cap, slab_off, slab_col,
-                                                                   slab_val, nnz_out, retry_rows, retry_count, flags);
+  k_num_warp_learned<LOGT, R32><<<blocks, wpb * 32, smem, lc.stream>>>(A, B, rows, nrows, cap, slab_off, slab_col,
+                                                                        slab_val, nnz_out, retry_rows, retry_count,
+                                                                        flags);
 }
 
 void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
@@ -868,10 +831,14 @@ void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int3
                              const LaunchCtx& lc, int wpb) {
   if (nrows == 0) return;
   const int w = wpb_for(log_t, wpb);
-#define SPG_NWL(L)                                                                                              \
-  case L:                                                                                                       \
-    num_warp_learned_one<L>(A, B, rows, nrows, cap, slab_off, slab_col, slab_val, nnz_out, retry_rows,          \
-                            retry_count, flags, lc, w);                                                         \
+#define SPG_NWL(L)                                                                                             \
+  case L:                                                                                                      \
+    if (B.rp32)                                                                                                \
+      num_warp_learned_one<L, true>(A, B, rows, nrows, cap, slab_off, slab_col, slab_val, nnz_out, retry_rows, \
+                                    retry_count, flags, lc, w);                                                \
+    else                                                                                                       \
+      num_warp_learned_one<L, false>(A, B, rows, nrows, cap, slab_off, slab_col, slab_val, nnz_out,            \
+                                     retry_rows, retry_count, flags, lc, w);                                   \
     break;
   switch (log_t) {
     SPG_NWL(5) SPG_NWL(6) SPG_NWL(7) SPG_NWL(8) SPG_NWL(9) SPG_NWL(10) SPG_NWL(11) SPG_NWL(12)
@@ -893,11 +860,7 @@ void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, in
                      const LaunchCtx& lc) {
   if (nheavy == 0) return;
   const size_t smem = (size_t)kTileWarps * (kTileCols + kTileWords + 32) * 4;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_num_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  cudaFuncSetAttribute(k_num_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_tile, kTileWarps * 32, smem);
   if (per_sm < 1) per_sm = 1;

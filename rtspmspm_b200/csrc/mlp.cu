@@ -9,6 +9,8 @@
 // the exact path, so results never depend on the network.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "mlp.hpp"
 
@@ -17,72 +19,83 @@ namespace spg {
 // Feature scaling: every feature is a log2 quantity divided by 16.
 constexpr float kFeatScale = 1.0f / 16.0f;
 
-// Features of row r of A*B (one warp per row):
+// Features of row r of A*B (computed by one warp, valid in every lane):
 //  0 log2(1 + |A_r|)               4 log2(1 + cols of B)
 //  1 log2(1 + products)            5 log2(1 + output column span)
 //  2 log2(1 + max touched |B_k|)   6 distinct fraction of a 32-product sample
 //  3 log2(1 + min touched |B_k|)   7 log2(1 + cols (1 - exp(-products/cols)))
-// Also writes the products (int64) of the row.
+// every log2 feature is scaled by 1/16.  Also returns the products.
+__device__ __forceinline__ int64_t row_features(const DCsr& A, const DCsr& B, int64_t r, float (&f)[kMlpIn]) {
+  const int lane = lane_id();
+  const int64_t s = A.rp[r], e = A.rp[r + 1];
+  const int64_t len = e - s;
+  int64_t sum = 0, mx = 0, mn = INT64_MAX;
+  int lo = 0x7fffffff, hi = -1;
+  for (int64_t p = s + lane; p < e; p += 32) {
+    const int32_t k = A.col[p];
+    const int64_t bs = B.rp[k], be = B.rp[k + 1];
+    const int64_t l = be - bs;
+    sum += l;
+    mx = l > mx ? l : mx;
+    mn = l < mn ? l : mn;
+    if (l > 0) {
+      lo = min(lo, B.col[bs]);
+      hi = max(hi, B.col[be - 1]);
+    }
+  }
+  sum = warp_sum(sum);
+  mx = warp_max(mx);
+  mn = warp_min(mn);
+  lo = warp_min(lo);
+  hi = warp_max(hi);
+  // sample: lane l takes A entry s + l*len/32 and a hashed position of its B row
+  int32_t j = -1 - lane;
+  bool valid = false;
+  if (len > 0 && lane < len) {
+    const int64_t p = s + (len <= 32 ? lane : (int64_t)lane * len / 32);
+    const int32_t k = A.col[p];
+    const int64_t bs = B.rp[k], be = B.rp[k + 1];
+    if (be > bs) {
+      const uint32_t hsh = (uint32_t)r * 2654435761u + (uint32_t)lane * 40503u;
+      j = B.col[bs + (int64_t)(hsh % (uint32_t)(be - bs))];
+      valid = true;
+    }
+  }
+  const unsigned vm = __ballot_sync(kFull, valid);
+  const unsigned grp = __match_any_sync(kFull, j);
+  const bool leader = valid && lane == __ffs(grp & vm) - 1;
+  const int distinct = __popc(__ballot_sync(kFull, leader));
+  const int nsample = __popc(vm);
+  if (mn == INT64_MAX) mn = 0;
+  const float cols = (float)B.cols;
+  const float span = hi >= lo ? (float)(hi - lo + 1) : 0.f;
+  const float fsum = (float)sum;
+  const float expect = cols > 0.f ? -cols * expm1f(-fsum / cols) : 0.f;
+  f[0] = log2f(1.f + (float)len) * kFeatScale;
+  f[1] = log2f(1.f + fsum) * kFeatScale;
+  f[2] = log2f(1.f + (float)mx) * kFeatScale;
+  f[3] = log2f(1.f + (float)mn) * kFeatScale;
+  f[4] = log2f(1.f + cols) * kFeatScale;
+  f[5] = log2f(1.f + span) * kFeatScale;
+  f[6] = nsample ? (float)distinct / (float)nsample : 0.f;
+  f[7] = log2f(1.f + expect) * kFeatScale;
+  return sum;
+}
+
 __global__ void k_features(DCsr A, DCsr B, float* feats, int64_t* prod) {
   const int lane = lane_id();
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = gw; r < A.rows; r += nw) {
-    const int64_t s = A.rp[r], e = A.rp[r + 1];
-    const int64_t len = e - s;
-    int64_t sum = 0, mx = 0, mn = INT64_MAX;
-    int lo = 0x7fffffff, hi = -1;
-    for (int64_t p = s + lane; p < e; p += 32) {
-      const int32_t k = A.col[p];
-      const int64_t bs = B.rp[k], be = B.rp[k + 1];
-      const int64_t l = be - bs;
-      sum += l;
-      mx = l > mx ? l : mx;
-      mn = l < mn ? l : mn;
-      if (l > 0) {
-        lo = min(lo, B.col[bs]);
-        hi = max(hi, B.col[be - 1]);
-      }
+    float f[kMlpIn];
+    const int64_t sum = row_features(A, B, r, f);
+    if (lane < kMlpIn) {
+      float v = f[0];
+#pragma unroll
+      for (int i = 1; i < kMlpIn; ++i) v = lane == i ? f[i] : v;
+      feats[r * kMlpIn + lane] = v;
     }
-    sum = warp_sum(sum);
-    mx = warp_max(mx);
-    mn = warp_min(mn);
-    lo = warp_min(lo);
-    hi = warp_max(hi);
-    // sample: lane l takes A entry s + l*len/32 and the middle of its B row
-    int32_t j = -1 - lane;
-    bool valid = false;
-    if (len > 0 && lane < len) {
-      const int64_t p = s + (len <= 32 ? lane : (int64_t)lane * len / 32);
-      const int32_t k = A.col[p];
-      const int64_t bs = B.rp[k], be = B.rp[k + 1];
-      if (be > bs) {
-        const uint32_t hsh = (uint32_t)r * 2654435761u + (uint32_t)lane * 40503u;
-        j = B.col[bs + (int64_t)(hsh % (uint32_t)(be - bs))];
-        valid = true;
-      }
-    }
-    const unsigned vm = __ballot_sync(kFull, valid);
-    const unsigned grp = __match_any_sync(kFull, j);
-    const bool leader = valid && lane == __ffs(grp & vm) - 1;
-    const int distinct = __popc(__ballot_sync(kFull, leader));
-    const int nsample = __popc(vm);
-    if (lane == 0) {
-      if (mn == INT64_MAX) mn = 0;
-      const double cols = (double)B.cols;
-      const double span = hi >= lo ? (double)(hi - lo + 1) : 0.0;
-      const double expect = cols > 0 ? cols * (1.0 - exp(-(double)sum / cols)) : 0.0;
-      float* f = feats + r * kMlpIn;
-      f[0] = log2f(1.f + (float)len) * kFeatScale;
-      f[1] = (float)log2(1.0 + (double)sum) * kFeatScale;
-      f[2] = log2f(1.f + (float)mx) * kFeatScale;
-      f[3] = log2f(1.f + (float)mn) * kFeatScale;
-      f[4] = (float)log2(1.0 + cols) * kFeatScale;
-      f[5] = (float)log2(1.0 + span) * kFeatScale;
-      f[6] = nsample ? (float)distinct / (float)nsample : 0.f;
-      f[7] = (float)log2(1.0 + expect) * kFeatScale;
-      if (prod) prod[r] = sum;
-    }
+    if (prod && lane == 0) prod[r] = sum;
   }
 }
 
@@ -101,77 +114,232 @@ __device__ __forceinline__ void load_params(const __nv_bfloat16* w, float* sw) {
   __syncthreads();
 }
 
-// Forward pass of one row; h1 kept in registers, h2 streamed into the output.
-// `sw` is read through a volatile pointer so the compiler re-reads the
-// weights per row instead of hoisting all 4,736 of them into registers.
-__device__ __forceinline__ void mlp_forward_row(const volatile float* sw, const float* x, float* h1, float* out) {
-#pragma unroll
-  for (int j = 0; j < kMlpHidden; ++j) {
-    float a = sw[kOffB1 + j];
-#pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) a += x[i] * sw[kOffW1 + i * kMlpHidden + j];
-    h1[j] = a > 0.f ? a : 0.f;
-  }
-  float o0 = sw[kOffB3 + 0], o1 = sw[kOffB3 + 1];
-#pragma unroll 1
-  for (int j = 0; j < kMlpHidden; ++j) {
-    float a = sw[kOffB2 + j];
-#pragma unroll
-    for (int i = 0; i < kMlpHidden; ++i) a += h1[i] * sw[kOffW2 + i * kMlpHidden + j];
-    a = a > 0.f ? a : 0.f;
-    o0 += a * sw[kOffW3 + j * kMlpOut + 0];
-    o1 += a * sw[kOffW3 + j * kMlpOut + 1];
-  }
-  out[0] = o0;
-  out[1] = o1;
+// ---------------------------------------------------------------------------
+// Tensor-core inference: the MLP on 16-row tiles with mma.sync m16n8k16
+// (BF16 operands, FP32 accumulation).  Weights live in shared memory
+// transposed (n-major, k contiguous) so each B fragment is one 32-bit load.
+// ---------------------------------------------------------------------------
+
+struct MlpSmem {
+  uint32_t w1t[kMlpHidden * 8];        // [n][k/2], k padded 8 -> 16
+  uint32_t w2t[kMlpHidden * 32];       // [n][k/2]
+  uint32_t w3t[8 * 32];                // [n][k/2], n padded 2 -> 8
+  float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpOut];
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
 }
 
-// Inference: predicted log2(1+nnz) and bin per row.
-__global__ void k_mlp_predict(const __nv_bfloat16* w, const float* feats, int64_t rows, float* out) {
-  extern __shared__ float sw[];
-  load_params(w, sw);
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
-    float x[kMlpIn], h1[kMlpHidden], o[kMlpOut];
-#pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) x[i] = feats[r * kMlpIn + i];
-    mlp_forward_row(sw, x, h1, o);
-    out[r * kMlpOut + 0] = o[0];
-    out[r * kMlpOut + 1] = o[1];
-  }
+__device__ __forceinline__ uint32_t pack_raw(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  const uint32_t l = *reinterpret_cast<const uint16_t*>(&lo);
+  const uint32_t h = *reinterpret_cast<const uint16_t*>(&hi);
+  return l | (h << 16);
 }
 
-// Inference fused with capacity sizing for the learned SpGEMM path.
-// cap = min(bound, ceil(margin * (2^o0 - 1)) + slack); a row is sent to the
-// exact path (need_exact = 1, cap = 0) when its cap exceeds the largest warp
-// table, its predicted bin says heavy, or force_overflow is set (cap = 1).
-__global__ void k_mlp_capacity(const __nv_bfloat16* w, const float* feats, const int64_t* prod, int64_t rows,
-                               int64_t cols, float margin, int slack, int64_t warp_cap, int force_overflow,
-                               int64_t* cap, uint8_t* need_exact) {
-  extern __shared__ float sw[];
-  load_params(w, sw);
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t p = prod[r];
-    const int64_t u = p < cols ? p : cols;
-    int64_t c = 0;
-    uint8_t ex = 0;
-    if (u > 0) {
-      float x[kMlpIn], h1[kMlpHidden], o[kMlpOut];
+__device__ __forceinline__ void load_mlp_smem(const __nv_bfloat16* w, MlpSmem& sm) {
+  const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
+  for (int i = threadIdx.x; i < kMlpHidden * 8; i += blockDim.x) {
+    const int n = i / 8, kp = i % 8;
+    const int k0 = 2 * kp, k1 = 2 * kp + 1;
+    const __nv_bfloat16 lo = k0 < kMlpIn ? w[kOffW1 + k0 * kMlpHidden + n] : z;
+    const __nv_bfloat16 hi = k1 < kMlpIn ? w[kOffW1 + k1 * kMlpHidden + n] : z;
+    sm.w1t[i] = pack_raw(lo, hi);
+  }
+  for (int i = threadIdx.x; i < kMlpHidden * 32; i += blockDim.x) {
+    const int n = i / 32, kp = i % 32;
+    sm.w2t[i] = pack_raw(w[kOffW2 + (2 * kp) * kMlpHidden + n], w[kOffW2 + (2 * kp + 1) * kMlpHidden + n]);
+  }
+  for (int i = threadIdx.x; i < 8 * 32; i += blockDim.x) {
+    const int n = i / 32, kp = i % 32;
+    sm.w3t[i] = n < kMlpOut ? pack_raw(w[kOffW3 + (2 * kp) * kMlpOut + n], w[kOffW3 + (2 * kp + 1) * kMlpOut + n]) : 0u;
+  }
+  for (int i = threadIdx.x; i < kMlpHidden; i += blockDim.x) {
+    sm.b1[i] = __bfloat162float(w[kOffB1 + i]);
+    sm.b2[i] = __bfloat162float(w[kOffB2 + i]);
+  }
+  if (threadIdx.x < kMlpOut) sm.b3[threadIdx.x] = __bfloat162float(w[kOffB3 + threadIdx.x]);
+  __syncthreads();
+}
+
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// MLP forward of a 16-row tile whose features sit in x (16 x 8, FP32).
+// On return, lanes with (lane & 3) == 0 hold: out[0..1] = (o0, o1) of row
+// lane/4 and out[2..3] = (o0, o1) of row lane/4 + 8.
+__device__ __forceinline__ void mlp_tile(const MlpSmem& sm, const float* x, float (&out)[4]) {
+  const int lane = lane_id();
+  const int g = lane >> 2, q = lane & 3;
+  uint32_t a[4];
+  a[0] = pack_bf16(x[g * kMlpIn + 2 * q], x[g * kMlpIn + 2 * q + 1]);
+  a[1] = pack_bf16(x[(g + 8) * kMlpIn + 2 * q], x[(g + 8) * kMlpIn + 2 * q + 1]);
+  a[2] = 0u;
+  a[3] = 0u;
+  float h[8][4];
 #pragma unroll
-      for (int i = 0; i < kMlpIn; ++i) x[i] = feats[r * kMlpIn + i];
-      mlp_forward_row(sw, x, h1, o);
-      const float lg = fminf(fmaxf(o[0], 0.f), 40.f);
-      double pred = exp2((double)lg) - 1.0;
-      double cd = ceil(pred * (double)margin) + (double)slack;
-      c = cd >= (double)u ? u : (int64_t)cd;
-      if (c < 1) c = 1;
-      if (force_overflow) c = 1;
-      if (c > warp_cap || o[1] > (float)(kMaxLogT + 0.5f)) {
-        ex = 1;
-        c = 0;
+  for (int nt = 0; nt < 8; ++nt) {
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    mma16816(d, a, sm.w1t[(nt * 8 + g) * 8 + q], 0u);
+    const int c = nt * 8 + 2 * q;
+    h[nt][0] = fmaxf(d[0] + sm.b1[c], 0.f);
+    h[nt][1] = fmaxf(d[1] + sm.b1[c + 1], 0.f);
+    h[nt][2] = fmaxf(d[2] + sm.b1[c], 0.f);
+    h[nt][3] = fmaxf(d[3] + sm.b1[c + 1], 0.f);
+  }
+  float h2[8][4];
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) h2[nt][0] = h2[nt][1] = h2[nt][2] = h2[nt][3] = 0.f;
+#pragma unroll
+  for (int kb = 0; kb < 4; ++kb) {
+    const uint32_t ak[4] = {pack_bf16(h[2 * kb][0], h[2 * kb][1]), pack_bf16(h[2 * kb][2], h[2 * kb][3]),
+                            pack_bf16(h[2 * kb + 1][0], h[2 * kb + 1][1]),
+                            pack_bf16(h[2 * kb + 1][2], h[2 * kb + 1][3])};
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+      mma16816(h2[nt], ak, sm.w2t[(nt * 8 + g) * 32 + kb * 8 + q], sm.w2t[(nt * 8 + g) * 32 + kb * 8 + 4 + q]);
+  }
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    const int c = nt * 8 + 2 * q;
+    h2[nt][0] = fmaxf(h2[nt][0] + sm.b2[c], 0.f);
+    h2[nt][1] = fmaxf(h2[nt][1] + sm.b2[c + 1], 0.f);
+    h2[nt][2] = fmaxf(h2[nt][2] + sm.b2[c], 0.f);
+    h2[nt][3] = fmaxf(h2[nt][3] + sm.b2[c + 1], 0.f);
+  }
+  float d3[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int kb = 0; kb < 4; ++kb) {
+    const uint32_t ak[4] = {pack_bf16(h2[2 * kb][0], h2[2 * kb][1]), pack_bf16(h2[2 * kb][2], h2[2 * kb][3]),
+                            pack_bf16(h2[2 * kb + 1][0], h2[2 * kb + 1][1]),
+                            pack_bf16(h2[2 * kb + 1][2], h2[2 * kb + 1][3])};
+    mma16816(d3, ak, sm.w3t[g * 32 + kb * 8 + q], sm.w3t[g * 32 + kb * 8 + 4 + q]);
+  }
+  out[0] = d3[0] + sm.b3[0];
+  out[1] = d3[1] + sm.b3[1];
+  out[2] = d3[2] + sm.b3[0];
+  out[3] = d3[3] + sm.b3[1];
+}
+
+constexpr int kPlanWarps = 8;
+
+// Inference on precomputed features: (log2(1+nnz), bin) per row.
+__global__ void __launch_bounds__(kPlanWarps * 32) k_mlp_predict(const __nv_bfloat16* w, const float* feats,
+                                                                 int64_t rows, float* out) {
+  __shared__ MlpSmem sm;
+  __shared__ float tile[kPlanWarps][16 * kMlpIn];
+  load_mlp_smem(w, sm);
+  const int lane = lane_id(), wib = threadIdx.x >> 5;
+  const int64_t ntiles = (rows + 15) / 16;
+  for (int64_t t = blockIdx.x * (int64_t)kPlanWarps + wib; t < ntiles; t += (int64_t)gridDim.x * kPlanWarps) {
+    const int64_t r0 = t * 16;
+    for (int i = lane; i < 16 * kMlpIn; i += 32) {
+      const int64_t r = r0 + i / kMlpIn;
+      tile[wib][i] = r < rows ? feats[r * kMlpIn + (i % kMlpIn)] : 0.f;
+    }
+    __syncwarp();
+    float o[4];
+    mlp_tile(sm, tile[wib], o);
+    if ((lane & 3) == 0) {
+      const int64_t ra = r0 + (lane >> 2), rb = ra + 8;
+      if (ra < rows) {
+        out[ra * kMlpOut + 0] = o[0];
+        out[ra * kMlpOut + 1] = o[1];
+      }
+      if (rb < rows) {
+        out[rb * kMlpOut + 0] = o[2];
+        out[rb * kMlpOut + 1] = o[3];
       }
     }
-    cap[r] = c;
-    need_exact[r] = ex;
+    __syncwarp();
+  }
+}
+
+// Capacity from a prediction: cap = min(bound, ceil(margin * (2^o0 - 1)) +
+// slack); a row goes to the exact path (need_exact = 1, cap = 0) when its
+// cap exceeds the largest warp table or its predicted bin says heavy;
+// force_overflow sets cap = 1 (every row then overflows and is re-run).
+__device__ __forceinline__ void capacity_of(int64_t p, int64_t cols, float o0, float o1, float margin, int slack,
+                                            int64_t warp_cap, int force_overflow, int64_t& cap, uint8_t& ex) {
+  const int64_t u = p < cols ? p : cols;
+  cap = 0;
+  ex = 0;
+  if (u <= 0) return;
+  const float lg = fminf(fmaxf(o0, 0.f), 40.f);
+  const double pred = exp2((double)lg) - 1.0;
+  const double cd = ceil(pred * (double)margin) + (double)slack;
+  int64_t c = cd >= (double)u ? u : (int64_t)cd;
+  if (c < 1) c = 1;
+  if (force_overflow) c = 1;
+  if (c > warp_cap || o1 > (float)kMaxLogT + 0.5f) {
+    ex = 1;
+    c = 0;
+  }
+  cap = c;
+}
+
+// Learned plan: per 16-row tile, the warp computes each row's features and
+// products, runs the MLP on the tile with tensor cores, and writes the
+// products, capacity and exact-path mark of every row.
+__global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B, const __nv_bfloat16* w,
+                                                                  float margin, int slack, int64_t warp_cap,
+                                                                  int force_overflow, int64_t* prod, int64_t* cap,
+                                                                  uint8_t* need_exact) {
+  __shared__ MlpSmem sm;
+  __shared__ float tile[kPlanWarps][16 * kMlpIn];
+  __shared__ int64_t tprod[kPlanWarps][16];
+  load_mlp_smem(w, sm);
+  const int lane = lane_id(), wib = threadIdx.x >> 5;
+  const int64_t rows = A.rows;
+  const int64_t ntiles = (rows + 15) / 16;
+  for (int64_t t = blockIdx.x * (int64_t)kPlanWarps + wib; t < ntiles; t += (int64_t)gridDim.x * kPlanWarps) {
+    const int64_t r0 = t * 16;
+    for (int i = 0; i < 16; ++i) {
+      const int64_t r = r0 + i;
+      float f[kMlpIn];
+      int64_t ps = 0;
+      if (r < rows) {
+        ps = row_features(A, B, r, f);
+      } else {
+#pragma unroll
+        for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < kMlpIn; ++k) tile[wib][i * kMlpIn + k] = f[k];
+        tprod[wib][i] = ps;
+      }
+    }
+    __syncwarp();
+    float o[4];
+    mlp_tile(sm, tile[wib], o);
+    if ((lane & 3) == 0) {
+      const int ia = lane >> 2, ib = ia + 8;
+      const int64_t ra = r0 + ia, rb = r0 + ib;
+      if (ra < rows) {
+        int64_t c;
+        uint8_t ex;
+        capacity_of(tprod[wib][ia], B.cols, o[0], o[1], margin, slack, warp_cap, force_overflow, c, ex);
+        prod[ra] = tprod[wib][ia];
+        cap[ra] = c;
+        need_exact[ra] = ex;
+      }
+      if (rb < rows) {
+        int64_t c;
+        uint8_t ex;
+        capacity_of(tprod[wib][ib], B.cols, o[2], o[3], margin, slack, warp_cap, force_overflow, c, ex);
+        prod[rb] = tprod[wib][ib];
+        cap[rb] = c;
+        need_exact[rb] = ex;
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -363,16 +531,18 @@ static int mlp_blocks(int64_t rows, int threads, int sms) {
 
 void launch_mlp_predict(const void* w16, const float* feats, int64_t rows, float* out, const LaunchCtx& lc) {
   if (rows == 0) return;
-  k_mlp_predict<<<mlp_blocks(rows, 128, lc.sms), 128, kMlpParams * sizeof(float), lc.stream>>>(
-      (const __nv_bfloat16*)w16, feats, rows, out);
+  const int64_t tiles = (rows + 15) / 16;
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((tiles + kPlanWarps - 1) / kPlanWarps, lc.sms * 8));
+  k_mlp_predict<<<blocks, kPlanWarps * 32, 0, lc.stream>>>((const __nv_bfloat16*)w16, feats, rows, out);
 }
 
-void launch_mlp_capacity(const void* w16, const float* feats, const int64_t* prod, int64_t rows, int64_t cols,
-                         float margin, int slack, int64_t warp_cap, int force_overflow, int64_t* cap,
-                         uint8_t* need_exact, const LaunchCtx& lc) {
-  if (rows == 0) return;
-  k_mlp_capacity<<<mlp_blocks(rows, 128, lc.sms), 128, kMlpParams * sizeof(float), lc.stream>>>(
-      (const __nv_bfloat16*)w16, feats, prod, rows, cols, margin, slack, warp_cap, force_overflow, cap, need_exact);
+void launch_learned_plan(const DCsr& A, const DCsr& B, const void* w16, float margin, int slack, int64_t warp_cap,
+                         int force_overflow, int64_t* prod, int64_t* cap, uint8_t* need_exact, const LaunchCtx& lc) {
+  if (A.rows == 0) return;
+  const int64_t tiles = (A.rows + 15) / 16;
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((tiles + kPlanWarps - 1) / kPlanWarps, lc.sms * 8));
+  k_learned_plan<<<blocks, kPlanWarps * 32, 0, lc.stream>>>(A, B, (const __nv_bfloat16*)w16, margin, slack, warp_cap,
+                                                            force_overflow, prod, cap, need_exact);
 }
 
 void launch_mlp_fwd_bwd(const void* w16, const float* feats, const float* targets, int64_t n, float* work,

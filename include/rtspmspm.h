@@ -181,6 +181,14 @@ spg_status spg_csr_copy(spg_ctx* ctx, const spg_csr* src, int32_t location, spg_
  */
 spg_status spg_csr_download(spg_ctx* ctx, const spg_csr* src, void* row_ptr, int32_t* col_idx, float* val);
 
+/*
+ * Copies rows rows[0..n) of a device matrix into a new host matrix (n rows,
+ * int64 row pointers, library-owned; release with spg_csr_free).  For
+ * inspecting parts of a product too large to copy whole.  No reference
+ * counterpart.
+ */
+spg_status spg_csr_extract_rows(spg_ctx* ctx, const spg_csr* src, const int64_t* rows, int64_t n, spg_csr* dst);
+
 /* ---- Matrix Market IO (host) --------------------------------------------- */
 
 /*

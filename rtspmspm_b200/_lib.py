@@ -109,6 +109,7 @@ SIGNATURES = [
     ("spg_csr_free", ctypes.c_int32, [_vp, _P(SpgCsr)]),
     ("spg_csr_copy", ctypes.c_int32, [_vp, _P(SpgCsr), ctypes.c_int32, _P(SpgCsr)]),
     ("spg_csr_download", ctypes.c_int32, [_vp, _P(SpgCsr), _vp, _vp, _vp]),
+    ("spg_csr_extract_rows", ctypes.c_int32, [_vp, _P(SpgCsr), _vp, ctypes.c_int64, _P(SpgCsr)]),
     ("spg_mtx_read", ctypes.c_int32, [ctypes.c_char_p, _P(SpgCsr)]),
     ("spg_mtx_write", ctypes.c_int32, [_vp, ctypes.c_char_p, _P(SpgCsr), ctypes.c_int32]),
     ("spg_mlp_load", ctypes.c_int32, [_vp, ctypes.c_char_p]),

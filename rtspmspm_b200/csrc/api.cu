@@ -742,4 +742,60 @@ spg_status spg_csr_download(spg_ctx* ctx, const spg_csr* src, void* row_ptr, int
   return SPG_OK;
 }
 
+spg_status spg_csr_extract_rows(spg_ctx* ctx, const spg_csr* src, const int64_t* rows, int64_t n, spg_csr* dst) {
+  if (!ctx || !src || !dst || n < 0 || (n > 0 && !rows)) return SPG_ERR_INVALID_ARG;
+  if (src->location != SPG_DEVICE) return fail(ctx, SPG_ERR_INVALID_ARG, "spg_csr_extract_rows needs a device matrix");
+  SPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int w = src->index_bits / 8;
+  std::vector<int64_t> start((size_t)n), len((size_t)n);
+  for (int64_t t = 0; t < n; ++t) {
+    if (rows[t] < 0 || rows[t] >= src->rows) return fail(ctx, SPG_ERR_INVALID_ARG, "row %lld out of range", (long long)rows[t]);
+    int64_t se[2] = {0, 0};
+    const char* base = static_cast<const char*>(src->row_ptr) + (size_t)rows[t] * w;
+    if (w == 8) {
+      SPG_CUDA(ctx, cudaMemcpy(se, base, 16, cudaMemcpyDeviceToHost));
+    } else {
+      int32_t s32[2];
+      SPG_CUDA(ctx, cudaMemcpy(s32, base, 8, cudaMemcpyDeviceToHost));
+      se[0] = s32[0];
+      se[1] = s32[1];
+    }
+    start[(size_t)t] = se[0];
+    len[(size_t)t] = se[1] - se[0];
+  }
+  int64_t total = 0;
+  for (int64_t t = 0; t < n; ++t) total += len[(size_t)t];
+  spg_csr d{};
+  d.rows = n;
+  d.cols = src->cols;
+  d.nnz = total;
+  d.capacity = total;
+  d.index_bits = 64;
+  d.location = SPG_HOST;
+  d.owner = 2;
+  d.row_ptr = malloc((size_t)(n + 1) * 8);
+  d.col_idx = (int32_t*)malloc(std::max<size_t>((size_t)total * 4, 4));
+  d.val = (float*)malloc(std::max<size_t>((size_t)total * 4, 4));
+  if (!d.row_ptr || !d.col_idx || !d.val) {
+    free(d.row_ptr);
+    free(d.col_idx);
+    free(d.val);
+    return fail(ctx, SPG_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+  int64_t* rp = static_cast<int64_t*>(d.row_ptr);
+  rp[0] = 0;
+  for (int64_t t = 0; t < n; ++t) {
+    rp[t + 1] = rp[t] + len[(size_t)t];
+    if (len[(size_t)t]) {
+      SPG_CUDA(ctx, cudaMemcpyAsync(d.col_idx + rp[t], src->col_idx + start[(size_t)t], (size_t)len[(size_t)t] * 4,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+      SPG_CUDA(ctx, cudaMemcpyAsync(d.val + rp[t], src->val + start[(size_t)t], (size_t)len[(size_t)t] * 4,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+    }
+  }
+  SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *dst = d;
+  return SPG_OK;
+}
+
 }  // extern "C"

@@ -417,10 +417,12 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
     p->R = R = R2;
     SPG_CUDA(ctx, cudaMemcpyAsync(p->row_mat, rm.data(), (size_t)std::max<int64_t>(R, 1) * 4, cudaMemcpyHostToDevice,
                                   ctx->stream));
-    SPG_CUDA(ctx, cudaMemcpyAsync(p->d_mats, p->mats.data(), (size_t)n * sizeof(BatchMat), cudaMemcpyHostToDevice,
-                                  ctx->stream));
     SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  // the descriptors now carry their final row starts and output offsets
+  SPG_CUDA(ctx, cudaMemcpyAsync(p->d_mats, p->mats.data(), (size_t)n * sizeof(BatchMat), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      kBatchArenaBytes));
   SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -142,6 +142,25 @@ class Result:
             L.spg_csr_free(self.engine.ctx, ctypes.byref(h))
         return Csr(int(h.rows), int(h.cols), rp, col, val)
 
+    def rows_to_host(self, rows) -> Csr:
+        """Copies only the given rows (a device C) into a host Csr."""
+        L = _lib.load()
+        sel = np.ascontiguousarray(rows, dtype=np.int64)
+        h = _lib.SpgCsr()
+        self.engine._check(L.spg_csr_extract_rows(self.engine.ctx, ctypes.byref(self.s), sel.ctypes.data,
+                                                  sel.size, ctypes.byref(h)))
+        try:
+            rp = np.ctypeslib.as_array(ctypes.cast(h.row_ptr, ctypes.POINTER(ctypes.c_int64)),
+                                       shape=(h.rows + 1,)).copy()
+            n = int(h.nnz)
+            col = np.ctypeslib.as_array(ctypes.cast(h.col_idx, ctypes.POINTER(ctypes.c_int32)), shape=(n,)).copy() \
+                if n else np.zeros(0, np.int32)
+            val = np.ctypeslib.as_array(ctypes.cast(h.val, ctypes.POINTER(ctypes.c_float)), shape=(n,)).copy() \
+                if n else np.zeros(0, np.float32)
+        finally:
+            L.spg_csr_free(self.engine.ctx, ctypes.byref(h))
+        return Csr(int(h.rows), int(h.cols), rp, col, val)
+
     def free(self) -> None:
         if self.s.owner and self.engine.ctx:
             _lib.load().spg_csr_free(self.engine.ctx, ctypes.byref(self.s))

@@ -1,0 +1,49 @@
+"""The spgemm CLI: same flags and contract as the reference executables
+(-m1 -m2 -o -l; one ms number in the log; exit 1 on failure)."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from rtspmspm_b200 import gen, read_mtx, write_mtx
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "rtspmspm_b200", "spgemm")
+
+
+def test_help_and_bad_flags_exit_1():
+    r = subprocess.run([CLI, "-h"], capture_output=True, text=True)
+    assert r.returncode == 1 and "--mat1" in r.stderr
+    r = subprocess.run([CLI, "--bogus"], capture_output=True, text=True)
+    assert r.returncode == 1
+
+
+def test_missing_input_exit_1(tmp_path):
+    r = subprocess.run([CLI, "-m1", str(tmp_path / "none.mtx")], capture_output=True, text=True)
+    assert r.returncode == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algo", ["plain", "learned", "cusparse"])
+def test_cli_end_to_end(tmp_path, algo):
+    A = gen.erdos_renyi(700, 500, 6.0, 8)
+    B = gen.erdos_renyi(500, 400, 5.0, 9)
+    pa, pb, pc, pl, pj = (str(tmp_path / n) for n in ("a.mtx", "b.mtx", "c.mtx", "log.txt", "r.json"))
+    write_mtx(pa, A)
+    write_mtx(pb, B)
+    r = subprocess.run([CLI, "-m1", pa, "-m2", pb, "-o", pc, "-l", pl, "--algo", algo, "--json", pj],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    ms = float(open(pl).read())
+    assert ms > 0
+    rep = json.load(open(pj))
+    assert rep["products"] == int(gen.row_products(A, B).sum())
+    C = read_mtx(pc)
+    R = oracle.spgemm(A, B)
+    np.testing.assert_array_equal(C.row_ptr, R.row_ptr)
+    np.testing.assert_array_equal(C.col_idx, R.col_idx)
+    if algo != "cusparse":
+        np.testing.assert_array_equal(C.val, R.val)  # shortest round-trip decimals

@@ -1,0 +1,147 @@
+"""Matrix Market reader/writer of the C ABI, checked against the reference's
+own reader/writer (cuSparse/src/util.cpp, built into oracle/_ref/) where
+available, and on tricky inputs."""
+import ctypes
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from rtspmspm_b200 import SpgError, gen, read_mtx, write_mtx
+from rtspmspm_b200.gen import coo_to_csr
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_UTIL = os.path.join(ROOT, "oracle", "_ref", "libref_util.so")
+REF_DATA = "/root/reference/optixSpMSpM/src/data"
+
+
+def ref_util():
+    if not os.path.exists(REF_UTIL):
+        pytest.skip("reference util not built (make -C oracle ref)")
+    L = ctypes.CDLL(REF_UTIL)
+    L.ref_read_coo.restype = ctypes.c_int64
+    L.ref_read_coo.argtypes = [ctypes.c_char_p] + [ctypes.c_void_p] * 5
+    L.ref_free.argtypes = [ctypes.c_void_p] * 3
+    L.ref_write_coo.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_int, ctypes.c_int, ctypes.c_int64]
+    return L
+
+
+def ref_read(path):
+    L = ref_util()
+    r, c, v = ctypes.POINTER(ctypes.c_int)(), ctypes.POINTER(ctypes.c_int)(), ctypes.POINTER(ctypes.c_float)()
+    nr, nc = ctypes.c_int(), ctypes.c_int()
+    n = L.ref_read_coo(path.encode(), ctypes.byref(r), ctypes.byref(c), ctypes.byref(v), ctypes.byref(nr),
+                       ctypes.byref(nc))
+    assert n >= 0
+    rr = np.ctypeslib.as_array(r, (n,)).copy() if n else np.zeros(0, np.int32)
+    cc = np.ctypeslib.as_array(c, (n,)).copy() if n else np.zeros(0, np.int32)
+    vv = np.ctypeslib.as_array(v, (n,)).copy() if n else np.zeros(0, np.float32)
+    L.ref_free(r, c, v)
+    return nr.value, nc.value, rr, cc, vv
+
+
+def test_roundtrip(tmp_path):
+    A = gen.erdos_renyi(300, 200, 5.0, 3)
+    p = str(tmp_path / "a.mtx")
+    write_mtx(p, A)
+    B = read_mtx(p)
+    assert (B.rows, B.cols) == (A.rows, A.cols)
+    np.testing.assert_array_equal(B.row_ptr, A.row_ptr)
+    np.testing.assert_array_equal(B.col_idx, A.col_idx)
+    np.testing.assert_array_equal(B.val, A.val)  # shortest round-trip decimal
+
+
+def test_writer_matches_reference_reader(tmp_path):
+    A = gen.rmat(9, 8, seed=1)
+    p = str(tmp_path / "a.mtx")
+    write_mtx(p, A)
+    nr, nc, r, c, v = ref_read(p)
+    assert (nr, nc) == (A.rows, A.cols)
+    B = coo_to_csr(nr, nc, r - 1, c - 1, v)
+    np.testing.assert_array_equal(B.row_ptr, A.row_ptr)
+    np.testing.assert_array_equal(B.col_idx, A.col_idx)
+    np.testing.assert_array_equal(B.val, A.val)
+
+
+def test_reader_matches_reference_on_reference_writer_output(tmp_path):
+    L = ref_util()
+    rng = np.random.default_rng(5)
+    r = rng.integers(1, 51, 400).astype(np.int32)
+    c = rng.integers(1, 41, 400).astype(np.int32)
+    keep = np.unique(r.astype(np.int64) * 100 + c, return_index=True)[1]
+    r, c = r[keep], c[keep]
+    v = rng.standard_normal(r.size).astype(np.float32)
+    p = str(tmp_path / "ref.mtx")
+    L.ref_write_coo(p.encode(), r.ctypes.data, c.ctypes.data, v.ctypes.data, 50, 40, r.size)
+    ours = read_mtx(p)
+    nr, nc, rr, cc, vv = ref_read(p)
+    ref = coo_to_csr(nr, nc, rr - 1, cc - 1, vv)
+    np.testing.assert_array_equal(ours.row_ptr, ref.row_ptr)
+    np.testing.assert_array_equal(ours.col_idx, ref.col_idx)
+    np.testing.assert_array_equal(ours.val, ref.val)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference fixtures not present")
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(REF_DATA, "*", "*_small.mtx"))))
+def test_reads_reference_fixtures_like_reference(path):
+    """Column-major, 1-based SuiteSparse subsets: same entries as the reference reader."""
+    ours = read_mtx(path)
+    nr, nc, r, c, v = ref_read(path)
+    ref = coo_to_csr(nr, nc, r - 1, c - 1, v, merge="sum")
+    assert (ours.rows, ours.cols) == (ref.rows, ref.cols)
+    np.testing.assert_array_equal(ours.row_ptr, ref.row_ptr)
+    np.testing.assert_array_equal(ours.col_idx, ref.col_idx)
+    np.testing.assert_allclose(ours.val, ref.val, rtol=1e-6)
+
+
+def test_symmetric_pattern_comments_duplicates(tmp_path):
+    p = tmp_path / "s.mtx"
+    p.write_text("%%MatrixMarket matrix coordinate pattern symmetric\n% comment\n\n4 4 4\n1 1\n3 1\n4 2\n3 1\n")
+    m = read_mtx(str(p))
+    d = m.to_scipy().toarray()
+    want = np.zeros((4, 4))
+    want[0, 0] = 1
+    want[2, 0] = want[0, 2] = 2  # the duplicate (3,1) is summed, then mirrored
+    want[3, 1] = want[1, 3] = 1
+    np.testing.assert_array_equal(d, want)
+
+
+def test_unsorted_real_general_sorted_on_read(tmp_path):
+    p = tmp_path / "u.mtx"
+    p.write_text("%%MatrixMarket matrix coordinate real general\n3 3 4\n3 3 1.5\n1 2 -2\n1 1 +3e0\n2 3 .25\n")
+    m = read_mtx(str(p))
+    np.testing.assert_array_equal(m.row_ptr, [0, 2, 3, 4])
+    np.testing.assert_array_equal(m.col_idx, [0, 1, 2, 2])
+    np.testing.assert_array_equal(m.val, np.array([3, -2, 0.25, 1.5], np.float32))
+
+
+@pytest.mark.parametrize("text,status", [
+    ("%%MatrixMarket matrix array real general\n2 2\n1\n2\n3\n4\n", 5),
+    ("%%MatrixMarket matrix coordinate real general\n2 2 3\n1 1 1\n2 2 2\n", 5),   # truncated
+    ("%%MatrixMarket matrix coordinate real general\n2 2 1\n3 1 1\n", 5),          # out of range
+    ("%%MatrixMarket matrix coordinate real general\n2 2 1\n1 x 1\n", 5),          # garbage
+])
+def test_malformed_files_rejected(tmp_path, text, status):
+    p = tmp_path / "bad.mtx"
+    p.write_text(text)
+    with pytest.raises(SpgError) as e:
+        read_mtx(str(p))
+    assert e.value.status == status
+
+
+def test_missing_file():
+    with pytest.raises(SpgError) as e:
+        read_mtx("/nonexistent/x.mtx")
+    assert e.value.status == 4
+
+
+def test_drop_zeros_writer(tmp_path):
+    m = coo_to_csr(2, 3, [0, 0, 1], [0, 2, 1], np.array([0.0, 1.0, 0.0], np.float32))
+    p = str(tmp_path / "z.mtx")
+    write_mtx(p, m, drop_zeros=True)
+    lines = open(p).read().split("\n")
+    assert lines[1] == "2 3 1" and lines[2] == "1 3 1"
+    write_mtx(p, m)
+    assert open(p).read().split("\n")[1] == "2 3 3"

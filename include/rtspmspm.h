@@ -166,6 +166,29 @@ spg_status spg_multiply(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_cs
 spg_status spg_multiply_batched(spg_ctx* ctx, int32_t n, const spg_csr* A, const spg_csr* B,
                                 spg_csr* C, const spg_opts* opts, spg_report* report);
 
+/*
+ * Allocation-free C = A * B, for callers that cannot let a library call
+ * cudaMalloc: processes whose device memory belongs to their own arena or
+ * budget, and hot paths that must not risk an allocation's latency or an
+ * out-of-memory failure mid-call.  No counterpart in the reference.
+ * A and B are device matrices with at most 262,144 rows each, and every
+ * output row must fit the warp hash tables (at most 2,048 intermediate
+ * products per row, capped at the column count); larger inputs are
+ * rejected with an error and a message in errbuf.  C carries caller-owned
+ * device buffers: row_ptr (rows+1 entries of C->index_bits width) and
+ * col_idx/val with C->capacity entries; on success C->nnz is set, and when
+ * the capacity is too small the call fails with C->nnz holding the size
+ * needed.  Runs on `stream` on the calling thread's current device.
+ * All scratch lives in one file-scope device array of about 9.3 MB that
+ * every GPU loading the library keeps until the process exits; the first
+ * call on a device looks up that array's address (make that first call
+ * before any stream capture).  Every call shares the array, so calls
+ * whose work overlaps on the GPU (other streams, other threads) race and
+ * must be serialized by the caller.
+ */
+spg_status spg_multiply_noalloc(void* stream, const spg_csr* A, const spg_csr* B, spg_csr* C,
+                                char* errbuf, int32_t errlen);
+
 /* Releases a matrix allocated by the library (owner != 0); no-op otherwise. */
 spg_status spg_csr_free(spg_ctx* ctx, spg_csr* m);
 

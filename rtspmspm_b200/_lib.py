@@ -106,6 +106,8 @@ SIGNATURES = [
     ("spg_multiply", ctypes.c_int32, [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
     ("spg_multiply_batched", ctypes.c_int32,
      [_vp, ctypes.c_int32, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
+    ("spg_multiply_noalloc", ctypes.c_int32,
+     [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), ctypes.c_char_p, ctypes.c_int32]),
     ("spg_csr_free", ctypes.c_int32, [_vp, _P(SpgCsr)]),
     ("spg_csr_copy", ctypes.c_int32, [_vp, _P(SpgCsr), ctypes.c_int32, _P(SpgCsr)]),
     ("spg_csr_download", ctypes.c_int32, [_vp, _P(SpgCsr), _vp, _vp, _vp]),

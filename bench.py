@@ -168,6 +168,100 @@ def reference_arm(args, A):
     return 0
 
 
+def other_workload(args) -> int:
+    """Per-method timings for the other configurations (1 GPU):
+    rmat20 = C=A*A on R-MAT scale 20 (a=.57, b=c=.19, edge factor 16, seed 0);
+    er4096 = C=A*A on the 4,096^2 Erdos-Renyi Poisson(8) matrix (seed 0);
+    batch512 = 512 independent uneven products (seed 1), one persistent
+    launch per stage replayed from a CUDA graph."""
+    import torch
+
+    from rtspmspm_b200 import DeviceCsr, Engine, _lib, gen
+
+    eng = Engine(0, use_torch_stream=True)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = {"workload": args.workload, "steps": args.steps, "warmup": args.warmup}
+
+    def timed(fn, k):
+        ts = []
+        for _ in range(k):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    if args.workload == "batch512":
+        pairs = gen.batch_uneven(count=512, seed=1)
+        dA = [DeviceCsr.from_host(a) for a, _ in pairs]
+        dB = [DeviceCsr.from_host(b) for _, b in pairs]
+        products = sum(int(gen.row_products(a, b).sum()) for a, b in pairs)
+        eng.tune(dA[:64], dB[:64], None)
+        for graph, tuned in ((True, True), (False, True), (True, False)):
+            for _ in range(args.warmup):
+                eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True)
+            holder = {}
+
+            def step():
+                res, rep = eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True)
+                holder["rep"] = rep
+
+            ms = timed(step, args.steps)
+            key = ("graph" if graph else "stream") + ("_tuned" if tuned else "_default")
+            out[key] = {"ms": round(ms, 3), "gflops": round(2 * products / ms / 1e6, 2),
+                        "nnz_c": holder["rep"]["nnz_c"], "kernel_launches": holder["rep"]["kernel_launches"]}
+        out.update({"products": products, "tuning": eng.get_tuning()})
+    else:
+        A = gen.rmat(20, 16, seed=0) if args.workload == "rmat20" else gen.erdos_renyi(4096, 4096, 8.0, 0)
+        dA = DeviceCsr.from_host(A)
+        products = int(gen.row_products(A, A).sum())
+        sa = dA.struct()
+        algos = ["plain", "learned"] + (["cusparse"] if args.workload == "er4096" else [])
+        for algo in algos:
+            o = eng.opts(algo=algo, skip_validation=True, stage_timing=False)
+            for _ in range(args.warmup):
+                c = _lib.SpgCsr()
+                eng.multiply_raw(sa, sa, o, c, _lib.SpgReport())
+                eng.free_raw(c)
+            holder = {}
+
+            def step():
+                c = _lib.SpgCsr()
+                rep = _lib.SpgReport()
+                eng.multiply_raw(sa, sa, o, c, rep)
+                holder["rep"] = rep
+                eng.free_raw(c)
+
+            ms = timed(step, args.steps)
+            o2 = eng.opts(algo=algo, skip_validation=True, stage_timing=True)
+            c = _lib.SpgCsr()
+            rep = _lib.SpgReport()
+            eng.multiply_raw(sa, sa, o2, c, rep)
+            eng.free_raw(c)
+            r = rep.as_dict()
+            out[algo] = {"ms": round(ms, 3), "gflops": round(2 * products / ms / 1e6, 2), "nnz_c": r["nnz_c"],
+                         "stages_ms": {k: round(v, 3) for k, v in r["stages_ms"].items()},
+                         "rows_predicted": r["rows_predicted"], "rows_overflow": r["rows_overflow"],
+                         "rows_heavy": r["rows_heavy"]}
+        out.update({"products": products, "rows": A.rows, "nnz_a": A.nnz})
+        if "plain" in out and "learned" in out:
+            out["speedup_learned_vs_plain"] = round(out["plain"]["ms"] / out["learned"]["ms"], 4)
+        if args.workload == "rmat20" and not args.no_cpu:
+            v, info = cpu_sample(A, args.cpu_seconds)
+            out["cpu_baseline"] = {"value": round(v, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
+                                   "sample": f"leading {info['rows']} rows ({info['products']} products, "
+                                             f"{info['seconds']:.1f} s)"}
+    print(json.dumps(out), flush=True)
+    eng.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -179,7 +273,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile", choices=["plain", "learned"], default=None,
                     help="only W warm-up + K steps of one method (short runs under ncu)")
+    ap.add_argument("--workload", choices=["stencil96", "rmat20", "er4096", "batch512"], default="stencil96",
+                    help="other configurations: one JSON line of per-method timings (not the headline)")
     args = ap.parse_args()
+    if args.workload != "stencil96":
+        return other_workload(args)
     args.warmup = max(args.warmup, 3)
 
     from rtspmspm_b200 import gen

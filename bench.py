@@ -198,11 +198,11 @@ def other_workload(args) -> int:
         return statistics.median(ts)
 
     if args.workload == "batch512":
-        pairs = gen.batch_uneven(count=512, seed=1)
+        pairs = gen.batch_uneven(count=args.batch_count, seed=1)
         dA = [DeviceCsr.from_host(a) for a, _ in pairs]
         dB = [DeviceCsr.from_host(b) for _, b in pairs]
         products = sum(int(gen.row_products(a, b).sum()) for a, b in pairs)
-        eng.tune(dA[:64], dB[:64], None)
+        eng.tune(dA[:min(64, len(dA))], dB[:min(64, len(dB))], None)
         for graph, tuned in ((True, True), (False, True), (True, False)):
             for _ in range(args.warmup):
                 eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True)
@@ -218,7 +218,7 @@ def other_workload(args) -> int:
                         "nnz_c": holder["rep"]["nnz_c"], "kernel_launches": holder["rep"]["kernel_launches"]}
         out.update({"products": products, "tuning": eng.get_tuning()})
     else:
-        A = gen.rmat(20, 16, seed=0) if args.workload == "rmat20" else gen.erdos_renyi(4096, 4096, 8.0, 0)
+        A = gen.rmat(args.rmat_scale, 16, seed=0) if args.workload == "rmat20" else gen.erdos_renyi(4096, 4096, 8.0, 0)
         dA = DeviceCsr.from_host(A)
         products = int(gen.row_products(A, A).sum())
         sa = dA.struct()
@@ -275,6 +275,8 @@ def main():
                     help="only W warm-up + K steps of one method (short runs under ncu)")
     ap.add_argument("--workload", choices=["stencil96", "rmat20", "er4096", "batch512"], default="stencil96",
                     help="other configurations: one JSON line of per-method timings (not the headline)")
+    ap.add_argument("--rmat-scale", type=int, default=20, help="scale of --workload rmat20 (smaller for profiling)")
+    ap.add_argument("--batch-count", type=int, default=512, help="products of --workload batch512")
     args = ap.parse_args()
     if args.workload != "stencil96":
         return other_workload(args)

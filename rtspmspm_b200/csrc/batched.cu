@@ -37,7 +37,9 @@ struct BatchMat {
 };
 
 constexpr int kBatchWarps = 8;
-constexpr int kBatchArenaBytes = 64 * 1024;
+constexpr int kBatchArenaSmall = 64 * 1024;    // tables up to 2^kBatchSplitLog slots
+constexpr int kBatchArenaLarge = 192 * 1024;   // larger tables
+constexpr int kBatchSplitLog = 10;
 constexpr int kRowsPerWarpTile = 4;
 
 // Products per global row and the bound min(products, cols_m).
@@ -76,17 +78,19 @@ __global__ void k_batch_bound_stats(const int32_t* row_mat, const int64_t* bound
   }
 }
 
-__device__ __forceinline__ int warps_usable(int logt, bool numeric) {
+__device__ __forceinline__ int warps_usable(int logt, bool numeric, int arena_bytes) {
   const int per_warp = (1 << logt) * (numeric ? 12 : 4);
-  int w = kBatchArenaBytes / per_warp;
+  int w = arena_bytes / per_warp;
   return w < 1 ? 1 : (w > kBatchWarps ? kBatchWarps : w);
 }
 
-// Persistent symbolic (NUMERIC = false) or numeric (true) stage over all warp
-// bins.  Tile t maps to (bin, first row) with the widest-table bins first.
+// Persistent symbolic (NUMERIC = false) or numeric (true) stage over the warp
+// bins [bin_lo, bin_hi].  Tile t maps to (bin, first row) with the
+// widest-table bins first.
 template <bool NUMERIC>
 __global__ void __launch_bounds__(kBatchWarps * 32) k_batch_rows(const BatchMat* mats, const int32_t* row_mat,
                                                                  const int32_t* lists, const int64_t* bin_off,
+                                                                 int bin_lo, int bin_hi, int arena_bytes,
                                                                  int64_t* nnz, const int64_t* gscan, int32_t* c_col,
                                                                  float* c_val, unsigned long long* ticket, int* flags) {
   extern __shared__ int32_t arena[];
@@ -95,8 +99,8 @@ __global__ void __launch_bounds__(kBatchWarps * 32) k_batch_rows(const BatchMat*
   const int lane = lane_id(), w = threadIdx.x >> 5;
   if (threadIdx.x < kNumWarpBins) {
     const int b = threadIdx.x;
-    const int64_t cnt = bin_off[b + 1] - bin_off[b];
-    const int64_t per = (int64_t)warps_usable(kMinLogT + b, NUMERIC) * kRowsPerWarpTile;
+    const int64_t cnt = (b >= bin_lo && b <= bin_hi) ? bin_off[b + 1] - bin_off[b] : 0;
+    const int64_t per = (int64_t)warps_usable(kMinLogT + b, NUMERIC, arena_bytes) * kRowsPerWarpTile;
     sh_tiles[b] = (cnt + per - 1) / per;
   }
   __syncthreads();
@@ -115,7 +119,7 @@ __global__ void __launch_bounds__(kBatchWarps * 32) k_batch_rows(const BatchMat*
     }
     if (bin < 0) break;
     const int logt = kMinLogT + bin;
-    const int usable = warps_usable(logt, NUMERIC);
+    const int usable = warps_usable(logt, NUMERIC, arena_bytes);
     const int64_t per = (int64_t)usable * kRowsPerWarpTile;
     const int64_t first = bin_off[bin] + t * per;
     const int64_t last = min(first + per, bin_off[bin + 1]);
@@ -137,8 +141,7 @@ __global__ void __launch_bounds__(kBatchWarps * 32) k_batch_rows(const BatchMat*
           switch (logt) {
 #define SPG_SYM(L)                                                                                    \
   case L:                                                                                             \
-    cnt = M.B.rp32 ? symbolic_row<L, true>(M.A, M.B, r, keys, ep, flags)                              \
-                   : symbolic_row<L, false>(M.A, M.B, r, keys, ep, flags);                            \
+    cnt = symbolic_row<L, true>(M.A, M.B, r, keys, ep, flags);                                       \
     break;
             SPG_SYM(5) SPG_SYM(6) SPG_SYM(7) SPG_SYM(8) SPG_SYM(9) SPG_SYM(10) SPG_SYM(11) SPG_SYM(12)
 #undef SPG_SYM
@@ -153,8 +156,7 @@ __global__ void __launch_bounds__(kBatchWarps * 32) k_batch_rows(const BatchMat*
           switch (logt) {
 #define SPG_NUM(L)                                                                                      \
   case L:                                                                                               \
-    if (M.B.rp32) numeric_row<L, true>(M.A, M.B, r, keys, vals, list, e2, c_col + off, c_val + off, want, flags); \
-    else numeric_row<L, false>(M.A, M.B, r, keys, vals, list, e2, c_col + off, c_val + off, want, flags);         \
+    numeric_row<L, true>(M.A, M.B, r, keys, vals, list, e2, c_col + off, c_val + off, want, flags);         \
     break;
             SPG_NUM(5) SPG_NUM(6) SPG_NUM(7) SPG_NUM(8) SPG_NUM(9) SPG_NUM(10) SPG_NUM(11) SPG_NUM(12)
 #undef SPG_NUM
@@ -275,24 +277,35 @@ void enqueue(spg_ctx* ctx, BatchPlan* p) {
   int64_t* cursors = p->binmeta + 2 * kNumBins + 1;
   launch_binning(p->bound, R, INT64_MAX, kBinSymbolic, bp, p->bin_of_row, counts, offsets, cursors, p->lists, lc);
   launches += 3;
-  const size_t smem = kBatchArenaBytes;
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_rows<false>, kBatchWarps * 32, smem);
-  const int grid_s = lc.sms * std::max(1, per_sm);
-  cudaMemsetAsync(ctx->d_counter + 4, 0, 16, lc.stream);
-  k_batch_rows<false><<<grid_s, kBatchWarps * 32, smem, lc.stream>>>(
-      p->d_mats, p->row_mat, p->lists, offsets, p->nnz, nullptr, nullptr, nullptr, ctx->d_counter + 4, ctx->d_flags);
-  ++launches;
+  // each stage: one persistent launch for small tables, one for large ones
+  auto stage = [&](bool numeric, unsigned long long* ticket) {
+    for (int part = 0; part < 2; ++part) {
+      const int lo = part == 0 ? 0 : kBatchSplitLog - kMinLogT + 1;
+      const int hi = part == 0 ? kBatchSplitLog - kMinLogT : kNumWarpBins - 1;
+      const int arena = part == 0 ? kBatchArenaSmall : kBatchArenaLarge;
+      int per_sm = 0;
+      if (numeric)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_rows<true>, kBatchWarps * 32, arena);
+      else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_rows<false>, kBatchWarps * 32, arena);
+      const int grid = lc.sms * std::max(1, per_sm);
+      cudaMemsetAsync(ticket + part, 0, 8, lc.stream);
+      if (numeric)
+        k_batch_rows<true><<<grid, kBatchWarps * 32, arena, lc.stream>>>(
+            p->d_mats, p->row_mat, p->lists, offsets, lo, hi, arena, p->nnz, p->nnz, p->c_col, p->c_val,
+            ticket + part, ctx->d_flags);
+      else
+        k_batch_rows<false><<<grid, kBatchWarps * 32, arena, lc.stream>>>(
+            p->d_mats, p->row_mat, p->lists, offsets, lo, hi, arena, p->nnz, nullptr, nullptr, nullptr,
+            ticket + part, ctx->d_flags);
+      ++launches;
+    }
+  };
+  stage(false, ctx->d_counter + 4);
   launch_binning(p->nnz, R, INT64_MAX, kBinNumeric, bp, p->bin_of_row, counts, offsets, cursors, p->lists, lc);
   launch_excl_scan(p->nnz, R, p->nnz, p->scan_tmp, lc);
   launches += 7;
-  per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_rows<true>, kBatchWarps * 32, smem);
-  const int grid_n = lc.sms * std::max(1, per_sm);
-  k_batch_rows<true><<<grid_n, kBatchWarps * 32, smem, lc.stream>>>(p->d_mats, p->row_mat, p->lists, offsets, p->nnz,
-                                                                    p->nnz, p->c_col, p->c_val, ctx->d_counter + 5,
-                                                                    ctx->d_flags);
-  ++launches;
+  stage(true, ctx->d_counter + 6);
   k_batch_finalize<<<blocks_for(R + p->n, 256), 256, 0, lc.stream>>>(p->d_mats, p->n, p->row_mat, R, p->nnz,
                                                                      p->rp_out, p->nnz_m);
   ++launches;
@@ -385,7 +398,8 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
   p->c_base.assign((size_t)n, 0);
   for (int m = 0; m < n; ++m) {
     BatchMat& M = p->mats[(size_t)m];
-    if ((int64_t)hmax[(size_t)m] > bp.warp_cap) {
+    // the persistent kernels use 32-bit row offsets of B (nnz(B) < 2^31)
+    if ((int64_t)hmax[(size_t)m] > bp.warp_cap || !M.B.rp32) {
       p->individual.push_back(m);
       // keep its rows out of the persistent stages: an empty A view
       M.A.rows = 0;
@@ -395,7 +409,7 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
     M.c_base = cbase;
     M.rp_base = rpbase;
     p->c_base[(size_t)m] = cbase;
-    if ((int64_t)hmax[(size_t)m] <= bp.warp_cap) cbase += (int64_t)hsum[(size_t)m];
+    if ((int64_t)hmax[(size_t)m] <= bp.warp_cap && M.B.rp32) cbase += (int64_t)hsum[(size_t)m];
     rpbase += A[m].rows + 1;
   }
   if (!p->individual.empty()) {
@@ -405,14 +419,13 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
     std::vector<int64_t> new_start((size_t)n, 0);
     for (int m = 0; m < n; ++m) {
       new_start[(size_t)m] = R2;
-      if (p->mats[(size_t)m].A.rows > 0 || (int64_t)hmax[(size_t)m] <= bp.warp_cap) R2 += A[m].rows;
+      if (p->mats[(size_t)m].A.rows > 0) R2 += A[m].rows;
     }
     std::vector<int32_t> rm((size_t)std::max<int64_t>(R2, 1));
     for (int m = 0; m < n; ++m) {
       BatchMat& M = p->mats[(size_t)m];
       M.row_start = new_start[(size_t)m];
-      if ((int64_t)hmax[(size_t)m] <= bp.warp_cap)
-        std::fill(rm.begin() + M.row_start, rm.begin() + M.row_start + A[m].rows, m);
+      if (M.A.rows > 0) std::fill(rm.begin() + M.row_start, rm.begin() + M.row_start + A[m].rows, m);
     }
     p->R = R = R2;
     SPG_CUDA(ctx, cudaMemcpyAsync(p->row_mat, rm.data(), (size_t)std::max<int64_t>(R, 1) * 4, cudaMemcpyHostToDevice,
@@ -424,9 +437,9 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
                                 ctx->stream));
   SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     kBatchArenaBytes));
+                                     kBatchArenaLarge));
   SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     kBatchArenaBytes));
+                                     kBatchArenaLarge));
   SPG_TRY(dmalloc(ctx, p, &p->nnz, (size_t)R + 1));
   SPG_TRY(dmalloc(ctx, p, &p->bin_of_row, (size_t)std::max<int64_t>(R, 1)));
   SPG_TRY(dmalloc(ctx, p, &p->binmeta, (size_t)(3 * kNumBins + 1)));
@@ -540,7 +553,7 @@ extern "C" spg_status spg_multiply_batched(spg_ctx* ctx, int32_t n, const spg_cs
     for (int m : plan->individual) report->rows += A[m].rows;
     report->rows_heavy = (int64_t)plan->individual.size();
     // products of the batched part (device sum)
-    unsigned long long* d = ctx->d_counter + 6;
+    unsigned long long* d = ctx->d_counter + 3;
     cudaMemsetAsync(d, 0, 8, ctx->stream);
     launch_sum(plan->prod, plan->R, d, launch_ctx(ctx));
     unsigned long long hp = 0;

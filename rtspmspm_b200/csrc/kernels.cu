@@ -464,6 +464,28 @@ __device__ __forceinline__ int64_t lower_bound_col(const int32_t* col, int64_t b
   return bs;
 }
 
+// Blocked index of B: for every row k of B and every column tile t,
+// bidx[k * (ntiles + 1) + t] = offset (from the row start) of the first
+// entry whose column is >= t * kTileCols.  One warp per row; every slot is
+// written exactly once.  Lets a heavy row's tile find the part of each B row
+// it needs with two loads instead of two binary searches.
+__global__ void k_build_blocked_index(DCsr B, int ntiles, int32_t* bidx) {
+  const int lane = lane_id();
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t k = gw; k < B.rows; k += nw) {
+    const int64_t s = B.rp[k], e = B.rp[k + 1];
+    int32_t* out = bidx + k * (int64_t)(ntiles + 1);
+    for (int64_t p = s + lane; p < e; p += 32) {
+      const int tcur = B.col[p] >> kTileShift;
+      const int tprev = p == s ? -1 : (B.col[p - 1] >> kTileShift);
+      for (int t = tprev + 1; t <= tcur; ++t) out[t] = (int32_t)(p - s);
+    }
+    const int tlast = e > s ? (B.col[e - 1] >> kTileShift) : -1;
+    for (int t = tlast + 1 + lane; t <= ntiles; t += 32) out[t] = (int32_t)(e - s);
+  }
+}
+
 // Per heavy row: exclusive scan of its tile counts (warp per row slot).
 __global__ void k_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
                                const int32_t* tile_cnt, int ntiles, int32_t* tile_off) {
@@ -492,7 +514,7 @@ __global__ void k_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const 
 __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, const int32_t* heavy_rows, int64_t nheavy,
                                                         const int32_t* big_slot, const int32_t* tile_cnt,
                                                         const int32_t* tile_off, int ntiles, const int64_t* c_rp,
-                                                        int32_t* c_col, float* c_val,
+                                                        int32_t* c_col, float* c_val, const int32_t* bidx,
                                                         unsigned long long* tile_counter, int* flags) {
   extern __shared__ uint32_t sm_tile[];
   const int lane = lane_id(), wib = threadIdx.x >> 5;
@@ -529,8 +551,14 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
         int64_t rs = B.rp[k], re = B.rp[k + 1];
         if (ntiles > 1 && re > rs) {
           // narrow to the tile's columns
-          if (B.col[rs] < c0) rs = lower_bound_col(B.col, rs, re, c0);
-          if (re > rs && B.col[re - 1] >= c1) re = lower_bound_col(B.col, rs, re, c1);
+          if (bidx) {
+            const int32_t* bi = bidx + (int64_t)k * (ntiles + 1) + tile;
+            re = rs + bi[1];
+            rs = rs + bi[0];
+          } else {
+            if (B.col[rs] < c0) rs = lower_bound_col(B.col, rs, re, c0);
+            if (re > rs && B.col[re - 1] >= c1) re = lower_bound_col(B.col, rs, re, c1);
+          }
         }
         bs = rs;
         len = (int)(re - rs);
@@ -854,9 +882,14 @@ void launch_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const int32_
                                                                                 ntiles, tile_off);
 }
 
+void launch_build_blocked_index(const DCsr& B, int ntiles, int32_t* bidx, const LaunchCtx& lc) {
+  if (B.rows == 0) return;
+  k_build_blocked_index<<<grid_for(B.rows, 256, 32, lc.sms * 16), 256, 0, lc.stream>>>(B, ntiles, bidx);
+}
+
 void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
                      const int32_t* tile_cnt, const int32_t* tile_off, int ntiles, const int64_t* c_rp,
-                     int32_t* c_col, float* c_val, unsigned long long* tile_counter, int* flags,
+                     int32_t* c_col, float* c_val, const int32_t* bidx, unsigned long long* tile_counter, int* flags,
                      const LaunchCtx& lc) {
   if (nheavy == 0) return;
   const size_t smem = (size_t)kTileWarps * (kTileCols + kTileWords + 32) * 4;
@@ -868,7 +901,7 @@ void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, in
   const int blocks = (int)std::min<int64_t>((tiles + kTileWarps - 1) / kTileWarps, (int64_t)lc.sms * per_sm);
   cudaMemsetAsync(tile_counter, 0, sizeof(unsigned long long), lc.stream);
   k_num_tile<<<blocks, kTileWarps * 32, smem, lc.stream>>>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off,
-                                                           ntiles, c_rp, c_col, c_val, tile_counter, flags);
+                                                           ntiles, c_rp, c_col, c_val, bidx, tile_counter, flags);
 }
 
 void launch_compact_rows(const int32_t* rows, int64_t nrows, const uint8_t* need_exact, const int64_t* slab_off,

@@ -177,7 +177,7 @@ __device__ __forceinline__ void sort_lookup_write(const int32_t* keys, const flo
   }
 }
 
-// Writes the row's n entries in column order (register sort up to 256
+// Writes the row's n entries in column order (register sort up to 512
 // entries, shared-memory bitonic sort of the list beyond that).
 template <int LOGT>
 __device__ __forceinline__ void emit_row(const int32_t* keys, const float* vals, int32_t* list, int n, int epoch,
@@ -191,6 +191,8 @@ __device__ __forceinline__ void emit_row(const int32_t* keys, const float* vals,
     sort_lookup_write<4, LOGT>(keys, vals, list, n, epoch, limit, out_col, out_val);
   } else if (n <= 256) {
     sort_lookup_write<8, LOGT>(keys, vals, list, n, epoch, limit, out_col, out_val);
+  } else if (T >= 1024 && n <= 512) {
+    sort_lookup_write<16, LOGT>(keys, vals, list, n, epoch, limit, out_col, out_val);
   } else {
     const int lane = lane_id();
     warp_sort_keys(list, n, T);

@@ -88,7 +88,7 @@ __device__ __forceinline__ int warps_usable(int logt, bool numeric, int arena_by
 // bins [bin_lo, bin_hi].  Tile t maps to (bin, first row) with the
 // widest-table bins first.
 template <bool NUMERIC>
-__global__ void __launch_bounds__(kBatchWarps * 32) k_batch_rows(const BatchMat* mats, const int32_t* row_mat,
+__global__ void __launch_bounds__(kBatchWarps * 32, 2) k_batch_rows(const BatchMat* mats, const int32_t* row_mat,
                                                                  const int32_t* lists, const int64_t* bin_off,
                                                                  int bin_lo, int bin_hi, int arena_bytes,
                                                                  int64_t* nnz, const int64_t* gscan, int32_t* c_col,

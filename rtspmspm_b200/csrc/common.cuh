@@ -16,7 +16,10 @@ namespace spg {
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int32_t kEmpty = -1;        // empty hash-table key
-constexpr int kTileShift = 13;        // heavy-row column tile: 8192 columns
+#ifndef SPG_TILE_SHIFT
+#define SPG_TILE_SHIFT 11
+#endif
+constexpr int kTileShift = SPG_TILE_SHIFT;  // heavy-row column tile: 2^11 = 2048 columns
 constexpr int kTileCols = 1 << kTileShift;
 constexpr int kTileWords = kTileCols / 32;
 
@@ -175,6 +178,57 @@ __device__ __forceinline__ int hash_find(const int32_t* keys, int log_t, int32_t
     s = (s + 1u) & mask;
   }
   return -1;
+}
+
+// B-row segments shorter than this are packed several to a warp step; longer
+// ones are read by the whole warp, one segment at a time.
+constexpr int kPackBelow = 16;
+
+// Visits every column c of the warp's 32 B-row segments [bs, bs + len) (one
+// per lane) in no particular order: f(c).  Segments of kPackBelow or more
+// entries are read by the whole warp, one at a time; shorter ones are packed
+// into steps of 32 consecutive entries, so short rows of B do not leave
+// lanes idle.
+template <typename Off, typename F>
+__device__ __forceinline__ void for_each_col(const int32_t* bcol, Off bs, int len, F&& f) {
+  const int lane = lane_id();
+  const bool is_long = len >= kPackBelow;
+  const unsigned long_mask = __ballot_sync(kFull, is_long);
+  for (unsigned m = long_mask; m; m &= m - 1) {
+    const int l = __ffs(m) - 1;
+    const Off sb = __shfl_sync(kFull, bs, l);
+    const int sl = __shfl_sync(kFull, len, l);
+    for (int q = lane; q < sl; q += 32) f(bcol[sb + q]);
+  }
+  const int sl = is_long ? 0 : len;
+  const int incl = warp_incl_scan(sl);
+  const int total = __shfl_sync(kFull, incl, 31);
+  const int excl = incl - sl;
+  for (int b0 = 0; b0 < total; b0 += 32) {
+    const int tt = b0 + lane;
+    const bool act = tt < total;
+    const int src = warp_upper_bound(incl, act ? tt : total - 1);
+    const Off sbs = __shfl_sync(kFull, bs, src);
+    const int sex = __shfl_sync(kFull, excl, src);
+    if (act) f(bcol[sbs + (Off)(tt - sex)]);
+  }
+}
+
+// Sum, in lane order, of the values `pr` of the lanes in `grp` (a group of
+// lanes sharing one output column, as found by __match_any_sync), started
+// from v.  Every lane of the warp must call it; lanes whose group is
+// theirs alone add just their own value.  Rounds = the largest group.
+__device__ __forceinline__ float group_sum_in_lane_order(unsigned grp, float pr, float v, bool use) {
+  const int rounds = (int)__reduce_max_sync(kFull, (unsigned)__popc(grp));
+  unsigned rest = grp;
+  for (int r = 0; r < rounds; ++r) {
+    const bool has = rest != 0u;
+    const int from = has ? __ffs(rest) - 1 : lane_id();
+    rest &= rest - 1u;
+    const float x = __shfl_sync(kFull, pr, from);
+    if (use && has) v = add_rn(v, x);
+  }
+  return v;
 }
 
 // Bitonic sort of 32*E keys held in registers, E per lane; element index =

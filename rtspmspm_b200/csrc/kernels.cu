@@ -260,31 +260,121 @@ __global__ void __launch_bounds__(512, 2) k_sym_warp(DCsr A, DCsr B, const int32
   }
 }
 
+// First lane l whose (nondecreasing) value v[l] exceeds t, for any integer
+// type; requires t < v[31].
+template <typename T>
+__device__ __forceinline__ int warp_upper_bound_t(T v, T t) {
+  int lo = 0;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    const T x = __shfl_sync(kFull, v, lo + s - 1);
+    if (x <= t) lo += s;
+  }
+  return lo;
+}
+
+// Visits every product column of `row` with the whole CTA (NTHR threads), in
+// no particular order: f(c).  A's row is taken NTHR entries at a time; a
+// CTA-wide exclusive scan of their B-row lengths goes to shared memory
+// (sh_excl[NTHR + 1], sh_bs[NTHR]) and the chunk's product stream is split
+// evenly among the warps.  A warp walks its share 32 products per step: a
+// window of the next 32 segment starts (one shared load per lane) and a
+// shuffle search give each lane its segment, so hub rows of B are spread
+// over every warp and short rows leave no lane idle.
+template <int NTHR, bool R32, typename F>
+__device__ __forceinline__ void cta_for_each_product(const DCsr& A, const DCsr& B, int32_t row,
+                                                     typename RowOff<R32>::T* sh_excl,
+                                                     typename RowOff<R32>::T* sh_bs,
+                                                     typename RowOff<R32>::T* sh_wsum, F&& f) {
+  using Off = typename RowOff<R32>::T;
+  constexpr int NW = NTHR / 32;
+  const int tid = threadIdx.x, lane = lane_id(), w = tid >> 5;
+  const int64_t s = A.rp[row], e = A.rp[row + 1];
+  for (int64_t c0 = s; c0 < e; c0 += NTHR) {
+    const int64_t p = c0 + tid;
+    Off bs = 0, len = 0;
+    if (p < e) {
+      const int32_t k = A.col[p];
+      bs = RowOff<R32>::at(B, k);
+      len = RowOff<R32>::at(B, k + 1) - bs;
+    }
+    const Off incl = warp_incl_scan(len);
+    if (lane == 31) sh_wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      const Off v = lane < NW ? sh_wsum[lane] : 0;
+      const Off iv = warp_incl_scan(v);
+      if (lane < NW) sh_wsum[lane] = iv - v;
+      if (lane == NW - 1) sh_wsum[NW] = iv;
+    }
+    __syncthreads();
+    sh_excl[tid] = incl - len + sh_wsum[w];
+    sh_bs[tid] = bs;
+    const int cnt = (int)min((int64_t)NTHR, e - c0);
+    const Off total = sh_wsum[NW];
+    if (tid == 0) sh_excl[cnt] = total;  // sentinel after the last entry
+    __syncthreads();
+    const Off lo = (Off)((int64_t)total * w / NW), hi = (Off)((int64_t)total * (w + 1) / NW);
+    if (lo < hi) {
+      // segment holding `lo`: sh_excl[i0] <= lo < sh_excl[i0 + 1]
+      int i0 = 0, i1 = cnt;
+      while (i1 - i0 > 1) {
+        const int mid = (i0 + i1) >> 1;
+        if (sh_excl[mid] <= lo) i0 = mid;
+        else i1 = mid;
+      }
+      int kc = i0;
+      for (Off pos = lo; pos < hi;) {
+        // starts of the segments after kc, kc + 1, ..., kc + 31
+        const int wi = kc + 1 + lane;
+        const Off nxt = wi <= cnt ? sh_excl[wi] : (Off)(R32 ? 0x7fffffff : INT64_MAX);
+        const Off wend = __shfl_sync(kFull, nxt, 31);
+        if (wend <= pos) {
+          // more than 31 empty segments in a row: slide the window on
+          kc += 31;
+          continue;
+        }
+        const Off lim = wend < hi ? wend : hi;
+        const Off x = pos + (Off)lane;
+        const bool act = x < lim;
+        const int l = warp_upper_bound_t<Off>(nxt, act ? x : pos);
+        const int i = kc + l;
+        if (act) f(B.col[sh_bs[i] + (x - sh_excl[i])]);
+        const int adv = (int)min((Off)32, lim - pos);
+        kc = __shfl_sync(kFull, i, adv - 1);
+        pos += adv;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // One CTA per row; CTA-wide key table of `table` slots (power of two).
 // Rows of this bin may become heavy in the numeric pass, so the per-tile
 // counts of their output columns are recorded too.
-__global__ void k_sym_block(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, int log_table, int64_t slot_base,
-                            int64_t* nnz_out, int32_t* big_slot, int32_t* tile_cnt, int ntiles, int* flags) {
+constexpr int kSymBlockThreads = 512;
+template <bool R32>
+__global__ void __launch_bounds__(kSymBlockThreads) k_sym_block(DCsr A, DCsr B, const int32_t* rows, int64_t nrows,
+                                                                int log_table, int64_t slot_base, int64_t* nnz_out,
+                                                                int32_t* big_slot, int32_t* tile_cnt, int ntiles,
+                                                                int* flags) {
+  using Off = typename RowOff<R32>::T;
   extern __shared__ int32_t sm_keys[];
+  __shared__ Off sh_excl[kSymBlockThreads + 1], sh_bs[kSymBlockThreads], sh_wsum[kSymBlockThreads / 32 + 1];
   __shared__ int sh_cnt;
   const int table = 1 << log_table;
-  const int lane = lane_id(), w = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int lane = lane_id();
   for (int s = threadIdx.x; s < table; s += blockDim.x) sm_keys[s] = kEmpty;
   for (int64_t idx = blockIdx.x; idx < nrows; idx += gridDim.x) {
     const int32_t row = rows[idx];
     if (threadIdx.x == 0) sh_cnt = 0;
     __syncthreads();
-    const int64_t s = A.rp[row], e = A.rp[row + 1];
     int cnt = 0;
-    for (int64_t p = s + w; p < e; p += nwarps) {
-      const int32_t k = A.col[p];
-      const int64_t bs = B.rp[k], be = B.rp[k + 1];
-      for (int64_t q = bs + lane; q < be; q += 32) {
-        bool fresh;
-        hash_insert(sm_keys, log_table, B.col[q], fresh, flags);
-        cnt += fresh;
-      }
-    }
+    cta_for_each_product<kSymBlockThreads, R32>(A, B, row, sh_excl, sh_bs, sh_wsum, [&](int32_t c) {
+      bool fresh;
+      hash_insert(sm_keys, log_table, c, fresh, flags);
+      cnt += fresh;
+    });
     cnt = warp_sum(cnt);
     if (lane == 0 && cnt) atomicAdd(&sh_cnt, cnt);
     __syncthreads();
@@ -307,9 +397,15 @@ __global__ void k_sym_block(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, 
 // One CTA per row; a bitmap over the row's column span in shared memory
 // (windows of `max_words` 32-bit words, a multiple of one tile).  Records
 // the per-tile counts for the heavy numeric pass.
-__global__ void k_sym_dense(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, int max_words, int64_t slot_base,
-                            int64_t* nnz_out, int32_t* big_slot, int32_t* tile_cnt, int ntiles, int* flags) {
+constexpr int kSymDenseThreads = 1024;
+template <bool R32>
+__global__ void __launch_bounds__(kSymDenseThreads) k_sym_dense(DCsr A, DCsr B, const int32_t* rows, int64_t nrows,
+                                                                int max_words, int64_t slot_base, int64_t* nnz_out,
+                                                                int32_t* big_slot, int32_t* tile_cnt, int ntiles,
+                                                                int* flags) {
+  using Off = typename RowOff<R32>::T;
   extern __shared__ uint32_t sm_bits[];
+  __shared__ Off sh_excl[kSymDenseThreads + 1], sh_bs[kSymDenseThreads], sh_wsum[kSymDenseThreads / 32 + 1];
   __shared__ int sh_lo, sh_hi;
   __shared__ unsigned long long sh_total;
   const int lane = lane_id(), w = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -326,7 +422,7 @@ __global__ void k_sym_dense(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, 
     int lo = 0x7fffffff, hi = -1;
     for (int64_t p = s + threadIdx.x; p < e; p += blockDim.x) {
       const int32_t k = A.col[p];
-      const int64_t bs = B.rp[k], be = B.rp[k + 1];
+      const Off bs = RowOff<R32>::at(B, k), be = RowOff<R32>::at(B, k + 1);
       if (be > bs) {
         lo = min(lo, B.col[bs]);
         hi = max(hi, B.col[be - 1]);
@@ -347,18 +443,12 @@ __global__ void k_sym_dense(DCsr A, DCsr B, const int32_t* rows, int64_t nrows, 
       const int nwords_tiles = ((nwords + kTileWords - 1) / kTileWords) * kTileWords;
       for (int t = threadIdx.x; t < nwords_tiles; t += blockDim.x) sm_bits[t] = 0u;
       __syncthreads();
-      for (int64_t p = s + w; p < e; p += nwarps) {
-        const int32_t k = A.col[p];
-        const int64_t bs = B.rp[k], be = B.rp[k + 1];
-        for (int64_t q = bs + lane; q < be; q += 32) {
-          const int32_t c = B.col[q];
-          if (c >= w0 && c < w1) {
-            const int off = (int)(c - w0);
-            atomicOr(&sm_bits[off >> 5], 1u << (off & 31));
-          }
+      cta_for_each_product<kSymDenseThreads, R32>(A, B, row, sh_excl, sh_bs, sh_wsum, [&](int32_t c) {
+        if (c >= w0 && c < w1) {
+          const int off = (int)(c - w0);
+          atomicOr(&sm_bits[off >> 5], 1u << (off & 31));
         }
-      }
-      __syncthreads();
+      });
       // per-tile popcounts: one warp per tile
       const int ntile_w = nwords_tiles / kTileWords;
       for (int tw = w; tw < ntile_w; tw += nwarps) {
@@ -505,17 +595,136 @@ __global__ void k_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const 
   }
 }
 
-// One warp per (heavy row, 8192-column tile).  The tile's products are taken
-// as one flattened stream in canonical order (k-major, then column), 32 per
-// step; products of different k that hit the same column inside a step are
-// grouped with __match_any_sync and added by the group's lowest lane in
-// lane order, so every output entry sees its products in canonical order.
-// Accumulator: dense tile of floats plus an occupancy bitmap.
+// Segments of at least this many entries are accumulated by the whole warp
+// without collision checks; shorter ones are packed.
+constexpr int kTileLongSeg = 16;
+
+// One segment (the part of B row k inside the tile, scaled by a).  Its
+// columns are distinct, so its products need no ordering among themselves:
+// lanes take 128 entries per round, issue all loads, then all accumulator
+// reads, then all writes.  `c0` is the tile's first column.
+template <typename Off>
+__device__ __forceinline__ void tile_segment(const DCsr& B, Off bs, int len, float a, int32_t c0, float* acc,
+                                             uint32_t* bits, int* flags) {
+  const int lane = lane_id();
+  for (int q0 = 0; q0 < len; q0 += 4 * 32) {
+    int32_t off[4];
+    float pr[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = q0 + u * 32 + lane;
+      off[u] = -1;
+      pr[u] = 0.f;
+      if (q < len) {
+        off[u] = B.col[bs + q] - c0;
+        pr[u] = prod_rn(a, B.val[bs + q]);
+      }
+    }
+    float cur[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) cur[u] = (uint32_t)off[u] < (uint32_t)kTileCols ? acc[off[u]] : 0.f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if ((uint32_t)off[u] < (uint32_t)kTileCols) {
+        acc[off[u]] = add_rn(cur[u], pr[u]);
+        atomicOr(&bits[off[u] >> 5], 1u << (off[u] & 31));
+      } else if (q0 + u * 32 + lane < len) {
+        raise_flag(flags, kFlagBadIndex);
+      }
+    }
+  }
+}
+
+// Segments of lanes [lo, hi) (all shorter than kTileLongSeg) taken as one
+// stream in canonical order (segment-major), 32 products per step, two steps
+// loaded at a time.  Products of one step that hit the same column (from
+// different segments) are grouped with __match_any_sync and added by the
+// group's lowest lane in lane order; steps without such a collision commit
+// directly.
+template <typename Off>
+__device__ __forceinline__ void tile_packed(const DCsr& B, Off bs, int len, float a, int lo, int hi, int32_t c0,
+                                            float* acc, uint32_t* bits, float* stage, int* flags) {
+  const int lane = lane_id();
+  const int lr = (lane >= lo && lane < hi) ? len : 0;
+  const int incl = warp_incl_scan(lr);
+  const int total = __shfl_sync(kFull, incl, 31);
+  const int excl = incl - lr;
+  for (int b0 = 0; b0 < total; b0 += 64) {
+    int32_t off[2];
+    float pr[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int tt = b0 + h * 32 + lane;
+      const bool act = tt < total;
+      const int src = warp_upper_bound(incl, act ? tt : total - 1);
+      const Off sbs = __shfl_sync(kFull, bs, src);
+      const int sex = __shfl_sync(kFull, excl, src);
+      const float sa = __shfl_sync(kFull, a, src);
+      off[h] = -1 - lane;  // unique dummy for idle lanes
+      pr[h] = 0.f;
+      if (act) {
+        const Off q = sbs + (Off)(tt - sex);
+        off[h] = B.col[q] - c0;
+        pr[h] = prod_rn(sa, B.val[q]);
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (b0 + h * 32 >= total) break;
+      const bool act = b0 + h * 32 + lane < total;
+      const unsigned grp = __match_any_sync(kFull, off[h]);
+      const bool inb = (uint32_t)off[h] < (uint32_t)kTileCols;
+      if (act && !inb) raise_flag(flags, kFlagBadIndex);
+      if (__all_sync(kFull, grp == (1u << lane))) {
+        if (act && inb) {
+          acc[off[h]] = add_rn(acc[off[h]], pr[h]);
+          atomicOr(&bits[off[h] >> 5], 1u << (off[h] & 31));
+        }
+      } else {
+        stage[lane] = pr[h];
+        __syncwarp();
+        if (act && inb && lane == __ffs(grp) - 1) {
+          float v = acc[off[h]];
+          for (unsigned g = grp; g; g &= g - 1) v = add_rn(v, stage[__ffs(g) - 1]);
+          acc[off[h]] = v;
+          atomicOr(&bits[off[h] >> 5], 1u << (off[h] & 31));
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Position of the r-th (0-based) set bit of w; requires r < popc(w).
+__device__ __forceinline__ int nth_set_bit(uint32_t w, int r) {
+  int pos = 0;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    const int c = __popc(w & ((1u << s) - 1u));
+    if (r >= c) {
+      r -= c;
+      w >>= s;
+      pos += s;
+    }
+  }
+  return pos;
+}
+
+// One warp per (heavy row, 2^kTileShift-column tile), tiles handed out by an atomic
+// ticket.  A's row is read 32 entries at a time (the next 32 loaded while the
+// current ones are processed); each entry's B row is narrowed to the tile
+// (blocked index, else binary search) and the segments are accumulated in
+// canonical order (k ascending, then column): long segments by the whole
+// warp, runs of short ones packed.  Accumulator: a dense tile of floats plus
+// an occupancy bitmap, emitted in column order with coalesced stores and
+// cleared as it is read.
+template <bool R32>
 __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, const int32_t* heavy_rows, int64_t nheavy,
                                                         const int32_t* big_slot, const int32_t* tile_cnt,
                                                         const int32_t* tile_off, int ntiles, const int64_t* c_rp,
                                                         int32_t* c_col, float* c_val, const int32_t* bidx,
                                                         unsigned long long* tile_counter, int* flags) {
+  using Off = typename RowOff<R32>::T;
   extern __shared__ uint32_t sm_tile[];
   const int lane = lane_id(), wib = threadIdx.x >> 5;
   float* acc = reinterpret_cast<float*>(sm_tile) + (size_t)wib * (kTileCols + kTileWords + 32);
@@ -537,98 +746,92 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
     const int want = tile_cnt[slot * ntiles + tile];
     if (want == 0) continue;
     const int64_t out = c_rp[row] + tile_off[slot * ntiles + tile];
-    const int64_t c0 = (int64_t)tile << kTileShift;
-    const int64_t c1 = c0 + kTileCols;
+    const int32_t c0 = tile << kTileShift;
+    const int64_t c1 = (int64_t)c0 + kTileCols;
     const int64_t s = A.rp[row], e = A.rp[row + 1];
+    int32_t k_nx = 0;
+    float a_nx = 0.f;
+    if (s + lane < e) {
+      k_nx = A.col[s + lane];
+      a_nx = A.val[s + lane];
+    }
     for (int64_t base = s; base < e; base += 32) {
-      const int64_t p = base + lane;
-      int64_t bs = 0;
+      const bool have = base + lane < e;
+      const int32_t k = k_nx;
+      const float a = a_nx;
+      if (base + 32 + lane < e) {
+        k_nx = A.col[base + 32 + lane];
+        a_nx = A.val[base + 32 + lane];
+      }
+      Off bs = 0;
       int len = 0;
-      float a = 0.f;
-      if (p < e) {
-        const int32_t k = A.col[p];
-        a = A.val[p];
-        int64_t rs = B.rp[k], re = B.rp[k + 1];
+      if (have) {
+        Off rs = RowOff<R32>::at(B, k), re = RowOff<R32>::at(B, k + 1);
         if (ntiles > 1 && re > rs) {
           // narrow to the tile's columns
           if (bidx) {
             const int32_t* bi = bidx + (int64_t)k * (ntiles + 1) + tile;
-            re = rs + bi[1];
-            rs = rs + bi[0];
+            re = rs + (Off)bi[1];
+            rs = rs + (Off)bi[0];
           } else {
-            if (B.col[rs] < c0) rs = lower_bound_col(B.col, rs, re, c0);
-            if (re > rs && B.col[re - 1] >= c1) re = lower_bound_col(B.col, rs, re, c1);
+            if (B.col[rs] < c0) rs = (Off)lower_bound_col(B.col, rs, re, c0);
+            if (re > rs && B.col[re - 1] >= c1) re = (Off)lower_bound_col(B.col, rs, re, c1);
           }
         }
         bs = rs;
         len = (int)(re - rs);
       }
-      const int incl = warp_incl_scan(len);
-      const int total = __shfl_sync(kFull, incl, 31);
-      const int excl = incl - len;
-      for (int b0 = 0; b0 < total; b0 += 32) {
-        const int tt = b0 + lane;
-        const bool act = tt < total;
-        const int src = warp_upper_bound(incl, act ? tt : total - 1);
-        const int64_t sbs = __shfl_sync(kFull, bs, src);
-        const int sex = __shfl_sync(kFull, excl, src);
-        const float sa = __shfl_sync(kFull, a, src);
-        int32_t j = -1 - lane;  // unique dummy for idle lanes
-        float pr = 0.f;
-        if (act) {
-          const int64_t q = sbs + (tt - sex);
-          j = B.col[q];
-          pr = prod_rn(sa, B.val[q]);
+      const int n = (int)min((int64_t)32, e - base);
+      const unsigned long_mask = __ballot_sync(kFull, len >= kTileLongSeg);
+      int idx = 0;
+      while (idx < n) {
+        if ((long_mask >> idx) & 1u) {
+          const Off sbs = __shfl_sync(kFull, bs, idx);
+          const int sl = __shfl_sync(kFull, len, idx);
+          const float sa = __shfl_sync(kFull, a, idx);
+          tile_segment(B, sbs, sl, sa, c0, acc, bits, flags);
+          __syncwarp();
+          ++idx;
+        } else {
+          const unsigned later = long_mask & (~0u << idx);
+          const int hi = later ? min(n, __ffs(later) - 1) : n;
+          tile_packed(B, bs, len, a, idx, hi, c0, acc, bits, stage, flags);
+          idx = hi;
         }
-        stage[lane] = pr;
-        const unsigned grp = __match_any_sync(kFull, j);
-        __syncwarp();
-        if (act && lane == __ffs(grp) - 1) {
-          const int off = (int)(j - c0);
-          if (off >= 0 && off < kTileCols) {
-            float v = acc[off];
-            unsigned g = grp;
-            while (g) {
-              const int m = __ffs(g) - 1;
-              g &= g - 1;
-              v = add_rn(v, stage[m]);
-            }
-            acc[off] = v;
-            atomicOr(&bits[off >> 5], 1u << (off & 31));
-          } else {
-            raise_flag(flags, kFlagBadIndex);
-          }
-        }
-        __syncwarp();
       }
     }
-    // extract in column order: lane owns words [lane*8, lane*8+8)
-    constexpr int kWPL = kTileWords / 32;
-    int cnt = 0;
-#pragma unroll
-    for (int x = 0; x < kWPL; ++x) cnt += __popc(bits[lane * kWPL + x]);
-    const int inc = warp_incl_scan(cnt);
-    const int tot = __shfl_sync(kFull, inc, 31);
-    if (tot != want && lane == 0) raise_flag(flags, kFlagCountDiff);
-    int64_t pos = out + (inc - cnt);
+    // emit in column order, 32 words (1024 columns) per round; lanes take
+    // consecutive entries, so the stores are coalesced
+    int64_t pos = out;
     const int64_t lim = out + want;
+    int found = 0;
 #pragma unroll 1
-    for (int x = 0; x < kWPL; ++x) {
-      const int wi = lane * kWPL + x;
-      uint32_t m = bits[wi];
-      bits[wi] = 0u;
-      while (m) {
-        const int bi = __ffs(m) - 1;
-        m &= m - 1;
-        const int off = wi * 32 + bi;
-        if (pos < lim) {
-          c_col[pos] = (int32_t)(c0 + off);
-          c_val[pos] = acc[off];
+    for (int g = 0; g < kTileWords; g += 32) {
+      const uint32_t wd = bits[g + lane];
+      const int c = __popc(wd);
+      const int inc = warp_incl_scan(c);
+      const int tot = __shfl_sync(kFull, inc, 31);
+      const int exc = inc - c;
+      for (int e0 = 0; e0 < tot; e0 += 32) {
+        const int ei = e0 + lane;
+        const bool act = ei < tot;
+        const int src = warp_upper_bound(inc, act ? ei : tot - 1);
+        const uint32_t sw = __shfl_sync(kFull, wd, src);
+        const int sex = __shfl_sync(kFull, exc, src);
+        if (act) {
+          const int off = ((g + src) << 5) + nth_set_bit(sw, ei - sex);
+          if (pos + ei < lim) {
+            c_col[pos + ei] = c0 + off;
+            c_val[pos + ei] = acc[off];
+          }
+          acc[off] = 0.f;
         }
-        acc[off] = 0.f;
-        ++pos;
       }
+      bits[g + lane] = 0u;
+      pos += tot;
+      found += tot;
     }
+    if (found != want && lane == 0) raise_flag(flags, kFlagCountDiff);
     __syncwarp();
   }
 }
@@ -639,9 +842,11 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
 
 // Copies each light row that did not overflow (need_exact == 0) from the
 // slab to its place in C; the row's length comes from C's row pointers.
-__global__ void k_compact_rows(const int32_t* rows, int64_t nrows, const uint8_t* need_exact, const int64_t* slab_off,
-                               const int32_t* slab_col, const float* slab_val, const int64_t* c_rp, int32_t* c_col,
-                               float* c_val) {
+// Lanes move 128 entries per round, all loads issued before the stores.
+__global__ void k_compact_rows(const int32_t* __restrict__ rows, int64_t nrows, const uint8_t* __restrict__ need_exact,
+                               const int64_t* __restrict__ slab_off, const int32_t* __restrict__ slab_col,
+                               const float* __restrict__ slab_val, const int64_t* __restrict__ c_rp,
+                               int32_t* __restrict__ c_col, float* __restrict__ c_val) {
   const int lane = lane_id();
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -649,11 +854,27 @@ __global__ void k_compact_rows(const int32_t* rows, int64_t nrows, const uint8_t
     const int32_t row = rows[idx];
     if (need_exact[row]) continue;
     const int64_t co = c_rp[row];
-    const int64_t n = c_rp[row + 1] - co;
+    const int n = (int)(c_rp[row + 1] - co);
     const int64_t so = slab_off[row];
-    for (int64_t t = lane; t < n; t += 32) {
-      c_col[co + t] = slab_col[so + t];
-      c_val[co + t] = slab_val[so + t];
+    for (int t0 = 0; t0 < n; t0 += 4 * 32) {
+      int32_t cc[4];
+      float vv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int t = t0 + u * 32 + lane;
+        if (t < n) {
+          cc[u] = slab_col[so + t];
+          vv[u] = slab_val[so + t];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int t = t0 + u * 32 + lane;
+        if (t < n) {
+          c_col[co + t] = cc[u];
+          c_val[co + t] = vv[u];
+        }
+      }
     }
   }
 }
@@ -775,30 +996,46 @@ void launch_sym_warp(int log_t, const DCsr& A, const DCsr& B, const int32_t* row
 #undef SPG_SW
 }
 
+template <bool R32>
+static void sym_block_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int log_table,
+                          int64_t slot_base, int64_t* nnz, int32_t* big_slot, int32_t* tile_cnt, int ntiles,
+                          int* flags, const LaunchCtx& lc) {
+  const size_t smem = ((size_t)1 << log_table) * sizeof(int32_t);
+  cudaFuncSetAttribute(k_sym_block<R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sym_block<R32>, kSymBlockThreads, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int blocks = (int)std::min<int64_t>(nrows, (int64_t)lc.sms * per_sm);
+  k_sym_block<R32><<<blocks, kSymBlockThreads, smem, lc.stream>>>(A, B, rows, nrows, log_table, slot_base, nnz, big_slot,
+                                                     tile_cnt, ntiles, flags);
+}
+
 void launch_sym_block(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int log_table,
                       int64_t slot_base, int64_t* nnz, int32_t* big_slot, int32_t* tile_cnt, int ntiles, int* flags,
                       const LaunchCtx& lc) {
   if (nrows == 0) return;
-  const size_t smem = ((size_t)1 << log_table) * sizeof(int32_t);
-  cudaFuncSetAttribute(k_sym_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sym_block, 512, smem);
-  if (per_sm < 1) per_sm = 1;
-  const int blocks = (int)std::min<int64_t>(nrows, (int64_t)lc.sms * per_sm);
-  k_sym_block<<<blocks, 512, smem, lc.stream>>>(A, B, rows, nrows, log_table, slot_base, nnz, big_slot, tile_cnt,
-                                                ntiles, flags);
+  if (B.rp32) sym_block_one<true>(A, B, rows, nrows, log_table, slot_base, nnz, big_slot, tile_cnt, ntiles, flags, lc);
+  else sym_block_one<false>(A, B, rows, nrows, log_table, slot_base, nnz, big_slot, tile_cnt, ntiles, flags, lc);
+}
+
+template <bool R32>
+static void sym_dense_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int64_t slot_base,
+                          int64_t* nnz, int32_t* big_slot, int32_t* tile_cnt, int ntiles, int* flags,
+                          const LaunchCtx& lc) {
+  const int max_words = kDenseWindowWords;
+  const size_t smem = (size_t)max_words * sizeof(uint32_t);
+  cudaFuncSetAttribute(k_sym_dense<R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int blocks = (int)std::min<int64_t>(nrows, (int64_t)lc.sms);
+  k_sym_dense<R32><<<blocks, kSymDenseThreads, smem, lc.stream>>>(A, B, rows, nrows, max_words, slot_base, nnz, big_slot,
+                                                      tile_cnt, ntiles, flags);
 }
 
 void launch_sym_dense(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int64_t slot_base,
                       int64_t* nnz, int32_t* big_slot, int32_t* tile_cnt, int ntiles, int* flags,
                       const LaunchCtx& lc) {
   if (nrows == 0) return;
-  const int max_words = kDenseWindowWords;
-  const size_t smem = (size_t)max_words * sizeof(uint32_t);
-  cudaFuncSetAttribute(k_sym_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int blocks = (int)std::min<int64_t>(nrows, (int64_t)lc.sms);
-  k_sym_dense<<<blocks, 1024, smem, lc.stream>>>(A, B, rows, nrows, max_words, slot_base, nnz, big_slot, tile_cnt,
-                                                 ntiles, flags);
+  if (B.rp32) sym_dense_one<true>(A, B, rows, nrows, slot_base, nnz, big_slot, tile_cnt, ntiles, flags, lc);
+  else sym_dense_one<false>(A, B, rows, nrows, slot_base, nnz, big_slot, tile_cnt, ntiles, flags, lc);
 }
 
 template <int LOGT, bool R32>
@@ -887,21 +1124,35 @@ void launch_build_blocked_index(const DCsr& B, int ntiles, int32_t* bidx, const 
   k_build_blocked_index<<<grid_for(B.rows, 256, 32, lc.sms * 16), 256, 0, lc.stream>>>(B, ntiles, bidx);
 }
 
+template <bool R32>
+static void num_tile_one(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy,
+                         const int32_t* big_slot, const int32_t* tile_cnt, const int32_t* tile_off, int ntiles,
+                         const int64_t* c_rp, int32_t* c_col, float* c_val, const int32_t* bidx,
+                         unsigned long long* tile_counter, int* flags, const LaunchCtx& lc) {
+  const size_t smem = (size_t)kTileWarps * (kTileCols + kTileWords + 32) * 4;
+  cudaFuncSetAttribute(k_num_tile<R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_tile<R32>, kTileWarps * 32, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int64_t tiles = nheavy * (int64_t)ntiles;
+  const int blocks = (int)std::min<int64_t>((tiles + kTileWarps - 1) / kTileWarps, (int64_t)lc.sms * per_sm);
+  cudaMemsetAsync(tile_counter, 0, sizeof(unsigned long long), lc.stream);
+  k_num_tile<R32><<<blocks, kTileWarps * 32, smem, lc.stream>>>(A, B, heavy_rows, nheavy, big_slot, tile_cnt,
+                                                                tile_off, ntiles, c_rp, c_col, c_val, bidx,
+                                                                tile_counter, flags);
+}
+
 void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
                      const int32_t* tile_cnt, const int32_t* tile_off, int ntiles, const int64_t* c_rp,
                      int32_t* c_col, float* c_val, const int32_t* bidx, unsigned long long* tile_counter, int* flags,
                      const LaunchCtx& lc) {
   if (nheavy == 0) return;
-  const size_t smem = (size_t)kTileWarps * (kTileCols + kTileWords + 32) * 4;
-  cudaFuncSetAttribute(k_num_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_tile, kTileWarps * 32, smem);
-  if (per_sm < 1) per_sm = 1;
-  const int64_t tiles = nheavy * (int64_t)ntiles;
-  const int blocks = (int)std::min<int64_t>((tiles + kTileWarps - 1) / kTileWarps, (int64_t)lc.sms * per_sm);
-  cudaMemsetAsync(tile_counter, 0, sizeof(unsigned long long), lc.stream);
-  k_num_tile<<<blocks, kTileWarps * 32, smem, lc.stream>>>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off,
-                                                           ntiles, c_rp, c_col, c_val, bidx, tile_counter, flags);
+  if (B.rp32)
+    num_tile_one<true>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off, ntiles, c_rp, c_col, c_val, bidx,
+                       tile_counter, flags, lc);
+  else
+    num_tile_one<false>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off, ntiles, c_rp, c_col, c_val, bidx,
+                        tile_counter, flags, lc);
 }
 
 void launch_compact_rows(const int32_t* rows, int64_t nrows, const uint8_t* need_exact, const int64_t* slab_off,

@@ -5,6 +5,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#ifndef SPG_TILE_SHIFT
+#define SPG_TILE_SHIFT 11
+#endif
+
 namespace spg {
 
 struct DCsr;
@@ -23,7 +27,11 @@ constexpr int kBinSymbolic = 0;
 constexpr int kBinNumeric = 1;
 constexpr int kBinLearned = 2;
 
-constexpr int kTileWarps = 6;              // warps per CTA of the heavy tile kernel
+// Warps per CTA of the heavy tile kernel: up to 8 per-warp tiles (floats,
+// bitmap, 32-float stage) within 227 KB of shared memory; the grid holds as
+// many CTAs per SM as fit.
+constexpr int kTileWarpBytes = ((1 << SPG_TILE_SHIFT) + (1 << SPG_TILE_SHIFT) / 32 + 32) * 4;
+constexpr int kTileWarps = (227 * 1024) / kTileWarpBytes > 8 ? 8 : (227 * 1024) / kTileWarpBytes;
 constexpr int kDenseWindowWords = 40960;   // 1,310,720 columns of bitmap per window
 
 struct BinParams {

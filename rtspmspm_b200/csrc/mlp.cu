@@ -19,83 +19,112 @@ namespace spg {
 // Feature scaling: every feature is a log2 quantity divided by 16.
 constexpr float kFeatScale = 1.0f / 16.0f;
 
-// Features of row r of A*B (computed by one warp, valid in every lane):
-//  0 log2(1 + |A_r|)               4 log2(1 + cols of B)
-//  1 log2(1 + products)            5 log2(1 + output column span)
-//  2 log2(1 + max touched |B_k|)   6 distinct fraction of a 32-product sample
-//  3 log2(1 + min touched |B_k|)   7 log2(1 + cols (1 - exp(-products/cols)))
-// every log2 feature is scaled by 1/16.  Also returns the products.
-__device__ __forceinline__ int64_t row_features(const DCsr& A, const DCsr& B, int64_t r, float (&f)[kMlpIn]) {
+// Integer statistics of row r of A*B, computed by one warp (valid in every
+// lane): |A_r|, products, max / min touched |B_k|, the output column span
+// [lo, hi] and a 32-product sample's distinct count.  The sample takes, per
+// lane l, A entry s + l (rows of at most 32 entries, folded into the main
+// pass) or s + l*len/32, and a hashed position of that entry's B row.
+struct RowStats {
+  int64_t len, sum, mx, mn;
+  int lo, hi;
+  int distinct, nsample;
+};
+
+template <bool R32>
+__device__ __forceinline__ RowStats row_stats(const DCsr& A, const DCsr& B, int64_t r) {
+  using Off = typename RowOff<R32>::T;
   const int lane = lane_id();
   const int64_t s = A.rp[r], e = A.rp[r + 1];
   const int64_t len = e - s;
-  int64_t sum = 0, mx = 0, mn = INT64_MAX;
+  const uint32_t hsh = (uint32_t)r * 2654435761u + (uint32_t)lane * 40503u;
+  Off sum = 0, mx = 0;
+  Off mn = R32 ? (Off)0x7fffffff : (Off)INT64_MAX;
   int lo = 0x7fffffff, hi = -1;
+  int32_t j = -1 - lane;
+  bool valid = false;
   for (int64_t p = s + lane; p < e; p += 32) {
     const int32_t k = A.col[p];
-    const int64_t bs = B.rp[k], be = B.rp[k + 1];
-    const int64_t l = be - bs;
+    const Off bs = RowOff<R32>::at(B, k), be = RowOff<R32>::at(B, k + 1);
+    const Off l = be - bs;
     sum += l;
     mx = l > mx ? l : mx;
     mn = l < mn ? l : mn;
     if (l > 0) {
       lo = min(lo, B.col[bs]);
       hi = max(hi, B.col[be - 1]);
+      if (len <= 32) {
+        j = B.col[bs + (Off)(hsh % (uint32_t)l)];
+        valid = true;
+      }
     }
   }
-  sum = warp_sum(sum);
-  mx = warp_max(mx);
-  mn = warp_min(mn);
-  lo = warp_min(lo);
-  hi = warp_max(hi);
-  // sample: lane l takes A entry s + l*len/32 and a hashed position of its B row
-  int32_t j = -1 - lane;
-  bool valid = false;
-  if (len > 0 && lane < len) {
-    const int64_t p = s + (len <= 32 ? lane : (int64_t)lane * len / 32);
+  if (len > 32) {
+    const int64_t p = s + (int64_t)lane * len / 32;
     const int32_t k = A.col[p];
-    const int64_t bs = B.rp[k], be = B.rp[k + 1];
+    const Off bs = RowOff<R32>::at(B, k), be = RowOff<R32>::at(B, k + 1);
     if (be > bs) {
-      const uint32_t hsh = (uint32_t)r * 2654435761u + (uint32_t)lane * 40503u;
-      j = B.col[bs + (int64_t)(hsh % (uint32_t)(be - bs))];
+      j = B.col[bs + (Off)(hsh % (uint32_t)(be - bs))];
       valid = true;
     }
   }
+  RowStats st;
+  if (R32) {
+    // a row's products are at most nnz(B) < 2^31
+    st.sum = (int64_t)__reduce_add_sync(kFull, (unsigned)sum);
+    st.mx = __reduce_max_sync(kFull, (int)mx);
+    st.mn = __reduce_min_sync(kFull, (int)mn);
+    if (st.mn == 0x7fffffff) st.mn = 0;
+  } else {
+    st.sum = warp_sum((int64_t)sum);
+    st.mx = warp_max((int64_t)mx);
+    st.mn = warp_min((int64_t)mn);
+    if (st.mn == INT64_MAX) st.mn = 0;
+  }
+  st.lo = __reduce_min_sync(kFull, lo);
+  st.hi = __reduce_max_sync(kFull, hi);
   const unsigned vm = __ballot_sync(kFull, valid);
   const unsigned grp = __match_any_sync(kFull, j);
   const bool leader = valid && lane == __ffs(grp & vm) - 1;
-  const int distinct = __popc(__ballot_sync(kFull, leader));
-  const int nsample = __popc(vm);
-  if (mn == INT64_MAX) mn = 0;
-  const float cols = (float)B.cols;
-  const float span = hi >= lo ? (float)(hi - lo + 1) : 0.f;
-  const float fsum = (float)sum;
-  const float expect = cols > 0.f ? -cols * expm1f(-fsum / cols) : 0.f;
-  f[0] = log2f(1.f + (float)len) * kFeatScale;
-  f[1] = log2f(1.f + fsum) * kFeatScale;
-  f[2] = log2f(1.f + (float)mx) * kFeatScale;
-  f[3] = log2f(1.f + (float)mn) * kFeatScale;
-  f[4] = log2f(1.f + cols) * kFeatScale;
-  f[5] = log2f(1.f + span) * kFeatScale;
-  f[6] = nsample ? (float)distinct / (float)nsample : 0.f;
-  f[7] = log2f(1.f + expect) * kFeatScale;
-  return sum;
+  st.distinct = __popc(__ballot_sync(kFull, leader));
+  st.nsample = __popc(vm);
+  st.len = len;
+  return st;
 }
 
+// Feature i of a row (i < 8); every log2 feature is scaled by 1/16:
+//  0 log2(1 + |A_r|)               4 log2(1 + cols of B)
+//  1 log2(1 + products)            5 log2(1 + output column span)
+//  2 log2(1 + max touched |B_k|)   6 distinct fraction of a 32-product sample
+//  3 log2(1 + min touched |B_k|)   7 log2(1 + cols (1 - exp(-products/cols)))
+__device__ __forceinline__ float feature_of(const RowStats& st, int64_t bcols, int i) {
+  const float cols = (float)bcols;
+  const float fsum = (float)st.sum;
+  if (i == 6) return st.nsample ? (float)st.distinct / (float)st.nsample : 0.f;
+  float x;
+  if (i == 7) {
+    x = cols > 0.f ? -cols * expm1f(-fsum / cols) : 0.f;
+  } else {
+    x = i == 0 ? (float)st.len
+      : i == 1 ? fsum
+      : i == 2 ? (float)st.mx
+      : i == 3 ? (float)st.mn
+      : i == 4 ? cols
+      : (st.hi >= st.lo ? (float)(st.hi - st.lo + 1) : 0.f);
+  }
+  return log2f(1.f + x) * kFeatScale;
+}
+
+// Features of every row of A*B (warp per row, lane i < 8 writes feature i),
+// plus the products per row when `prod` is set.
+template <bool R32>
 __global__ void k_features(DCsr A, DCsr B, float* feats, int64_t* prod) {
   const int lane = lane_id();
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = gw; r < A.rows; r += nw) {
-    float f[kMlpIn];
-    const int64_t sum = row_features(A, B, r, f);
-    if (lane < kMlpIn) {
-      float v = f[0];
-#pragma unroll
-      for (int i = 1; i < kMlpIn; ++i) v = lane == i ? f[i] : v;
-      feats[r * kMlpIn + lane] = v;
-    }
-    if (prod && lane == 0) prod[r] = sum;
+    const RowStats st = row_stats<R32>(A, B, r);
+    if (lane < kMlpIn) feats[r * kMlpIn + lane] = feature_of(st, B.cols, lane);
+    if (prod && lane == 0) prod[r] = st.sum;
   }
 }
 
@@ -287,6 +316,7 @@ __device__ __forceinline__ void capacity_of(int64_t p, int64_t cols, float o0, f
 // Learned plan: per 16-row tile, the warp computes each row's features and
 // products, runs the MLP on the tile with tensor cores, and writes the
 // products, capacity and exact-path mark of every row.
+template <bool R32>
 __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B, const __nv_bfloat16* w,
                                                                   float margin, int slack, int64_t warp_cap,
                                                                   int force_overflow, int64_t* prod, int64_t* cap,
@@ -302,18 +332,13 @@ __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B
     const int64_t r0 = t * 16;
     for (int i = 0; i < 16; ++i) {
       const int64_t r = r0 + i;
-      float f[kMlpIn];
-      int64_t ps = 0;
       if (r < rows) {
-        ps = row_features(A, B, r, f);
+        const RowStats st = row_stats<R32>(A, B, r);
+        if (lane < kMlpIn) tile[wib][i * kMlpIn + lane] = feature_of(st, B.cols, lane);
+        if (lane == 0) tprod[wib][i] = st.sum;
       } else {
-#pragma unroll
-        for (int k = 0; k < kMlpIn; ++k) f[k] = 0.f;
-      }
-      if (lane == 0) {
-#pragma unroll
-        for (int k = 0; k < kMlpIn; ++k) tile[wib][i * kMlpIn + k] = f[k];
-        tprod[wib][i] = ps;
+        if (lane < kMlpIn) tile[wib][i * kMlpIn + lane] = 0.f;
+        if (lane == 0) tprod[wib][i] = 0;
       }
     }
     __syncwarp();
@@ -519,7 +544,8 @@ void launch_features(const DCsr& A, const DCsr& B, float* feats, int64_t* prod, 
   if (A.rows == 0) return;
   int64_t blocks = (A.rows * 32 + 255) / 256;
   if (blocks > lc.sms * 16) blocks = lc.sms * 16;
-  k_features<<<(unsigned)blocks, 256, 0, lc.stream>>>(A, B, feats, prod);
+  if (B.rp32) k_features<true><<<(unsigned)blocks, 256, 0, lc.stream>>>(A, B, feats, prod);
+  else k_features<false><<<(unsigned)blocks, 256, 0, lc.stream>>>(A, B, feats, prod);
 }
 
 static int mlp_blocks(int64_t rows, int threads, int sms) {
@@ -541,8 +567,12 @@ void launch_learned_plan(const DCsr& A, const DCsr& B, const void* w16, float ma
   if (A.rows == 0) return;
   const int64_t tiles = (A.rows + 15) / 16;
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((tiles + kPlanWarps - 1) / kPlanWarps, lc.sms * 8));
-  k_learned_plan<<<blocks, kPlanWarps * 32, 0, lc.stream>>>(A, B, (const __nv_bfloat16*)w16, margin, slack, warp_cap,
-                                                            force_overflow, prod, cap, need_exact);
+  if (B.rp32)
+    k_learned_plan<true><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(A, B, (const __nv_bfloat16*)w16, margin, slack,
+                                                                    warp_cap, force_overflow, prod, cap, need_exact);
+  else
+    k_learned_plan<false><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(A, B, (const __nv_bfloat16*)w16, margin, slack,
+                                                                     warp_cap, force_overflow, prod, cap, need_exact);
 }
 
 void launch_mlp_fwd_bwd(const void* w16, const float* feats, const float* targets, int64_t n, float* work,

@@ -56,6 +56,8 @@ __device__ __forceinline__ int table_find(const int32_t* keys, int log_t, int32_
 
 // Exact number of distinct output columns of `row` (keys-only table).
 // epoch >= 0: epoch-tagged table; kNoEpoch: plain keys, cleared here.
+// A's row is taken 32 entries at a time; long B rows are read by the whole
+// warp, short ones packed (for_each_col).
 template <int LOGT, bool R32>
 __device__ __forceinline__ int symbolic_row(const DCsr& A, const DCsr& B, int32_t row, int32_t* keys, int epoch,
                                             int* flags) {
@@ -73,16 +75,11 @@ __device__ __forceinline__ int symbolic_row(const DCsr& A, const DCsr& B, int32_
       bs = RowOff<R32>::at(B, k);
       len = (int)(RowOff<R32>::at(B, k + 1) - bs);
     }
-    const int n = (int)min((int64_t)32, e - base);
-    for (int t = 0; t < n; ++t) {
-      const Off bst = __shfl_sync(kFull, bs, t);
-      const int l = __shfl_sync(kFull, len, t);
-      for (int q = lane; q < l; q += 32) {
-        bool fresh;
-        if (table_insert(keys, LOGT, B.col[bst + q], epoch, fresh) < 0) raise_flag(flags, kFlagHashFull);
-        cnt += fresh;
-      }
-    }
+    for_each_col(B.col, bs, len, [&](int32_t c) {
+      bool fresh;
+      if (table_insert(keys, LOGT, c, epoch, fresh) < 0) raise_flag(flags, kFlagHashFull);
+      cnt += fresh;
+    });
   }
   __syncwarp();
   cnt = warp_sum(cnt);
@@ -93,19 +90,104 @@ __device__ __forceinline__ int symbolic_row(const DCsr& A, const DCsr& B, int32_
   return cnt;
 }
 
-// Accumulates row `row` in canonical order: k-serial (one B row at a time),
-// lanes parallel over the columns of B_k.  Within one B row all columns are
-// distinct, so each slot receives at most one product per step and
-// __syncwarp orders the steps.  New columns are appended to `list` in the
-// order they are first seen; returns their number, or -1 when LEARNED and
-// more than `cap` distinct columns appear or the table fills (the learned
-// path's overflow).
+// Records a step's new columns in the first-seen list.  Returns false when
+// LEARNED and the step overflows the capacity or the table (the learned
+// path's overflow); otherwise a full table raises kFlagHashFull.
+template <bool LEARNED>
+__device__ __forceinline__ bool record_step(bool fresh, bool failed, int32_t j, int32_t* list, int cap, int& count,
+                                            int* flags) {
+  const unsigned m = __ballot_sync(kFull, fresh);
+  if (LEARNED) {
+    if (__any_sync(kFull, failed) || count + __popc(m) > cap) {
+      __syncwarp();
+      return false;
+    }
+  } else if (failed) {
+    raise_flag(flags, kFlagHashFull);
+  }
+  if (fresh) list[count + __popc(m & ((1u << lane_id()) - 1u))] = j;
+  count += __popc(m);
+  __syncwarp();
+  return true;
+}
+
+// One segment (B row k scaled by a), k-serial: lanes over its columns, 32 per
+// step.  Its columns are distinct, so each slot gets at most one product per
+// step and __syncwarp orders the steps.
+template <int LOGT, bool LEARNED, typename Off>
+__device__ __forceinline__ bool acc_segment(const DCsr& B, Off bs, int len, float a, int32_t* keys, float* vals,
+                                            int32_t* list, int epoch, int cap, int& count, int* flags) {
+  const int lane = lane_id();
+  for (int q0 = 0; q0 < len; q0 += 32) {
+    const int q = q0 + lane;
+    bool fresh = false, failed = false;
+    int32_t j = 0;
+    if (q < len) {
+      j = B.col[bs + q];
+      const float pr = prod_rn(a, B.val[bs + q]);
+      const int slot = table_insert(keys, LOGT, j, epoch, fresh);
+      if (slot < 0) failed = true;
+      else vals[slot] = add_rn(fresh ? 0.f : vals[slot], pr);
+    }
+    if (!record_step<LEARNED>(fresh, failed, j, list, cap, count, flags)) return false;
+  }
+  return true;
+}
+
+// Segments of lanes [lo, hi) (all shorter than kPackBelow) taken as one
+// stream in canonical order (segment-major), 32 products per step.  Products
+// of one step that hit the same column (from different segments) are grouped
+// with __match_any_sync; the group's lowest lane inserts the column and adds
+// the group's products in lane order, so every entry still sees its products
+// in canonical order.
+template <int LOGT, bool LEARNED, typename Off>
+__device__ __forceinline__ bool acc_packed(const DCsr& B, Off bs, int len, float a, int lo, int hi, int32_t* keys,
+                                           float* vals, int32_t* list, int epoch, int cap, int& count, int* flags) {
+  const int lane = lane_id();
+  const int lr = (lane >= lo && lane < hi) ? len : 0;
+  const int incl = warp_incl_scan(lr);
+  const int total = __shfl_sync(kFull, incl, 31);
+  const int excl = incl - lr;
+  for (int b0 = 0; b0 < total; b0 += 32) {
+    const int tt = b0 + lane;
+    const bool act = tt < total;
+    const int src = warp_upper_bound(incl, act ? tt : total - 1);
+    const Off sbs = __shfl_sync(kFull, bs, src);
+    const int sex = __shfl_sync(kFull, excl, src);
+    const float sa = __shfl_sync(kFull, a, src);
+    int32_t j = -1 - lane;  // unique dummy for idle lanes
+    float pr = 0.f;
+    if (act) {
+      const Off q = sbs + (Off)(tt - sex);
+      j = B.col[q];
+      pr = prod_rn(sa, B.val[q]);
+    }
+    const unsigned grp = __match_any_sync(kFull, j);
+    const bool leader = act && (grp & ((1u << lane) - 1u)) == 0u;
+    bool fresh = false;
+    int slot = -1;
+    if (leader) slot = table_insert(keys, LOGT, j, epoch, fresh);
+    const bool ok = leader && slot >= 0;
+    float v = (ok && !fresh) ? vals[slot] : 0.f;
+    v = group_sum_in_lane_order(grp, pr, v, ok);
+    if (ok) vals[slot] = v;
+    if (!record_step<LEARNED>(fresh, leader && slot < 0, j, list, cap, count, flags)) return false;
+  }
+  return true;
+}
+
+// Accumulates row `row` in canonical order (k ascending through A's row,
+// then column ascending through B's row k).  A's row is taken 32 entries at
+// a time: B rows of kPackBelow or more entries go k-serially
+// (acc_segment), runs of shorter ones are packed (acc_packed).  New columns
+// are appended to `list` in the order they are first seen; returns their
+// number, or -1 when LEARNED and more than `cap` distinct columns appear or
+// the table fills (the learned path's overflow).
 template <int LOGT, bool R32, bool LEARNED>
 __device__ __forceinline__ int accumulate_row(const DCsr& A, const DCsr& B, int32_t row, int32_t* keys, float* vals,
                                               int32_t* list, int epoch, int cap, int* flags) {
   using Off = typename RowOff<R32>::T;
   const int lane = lane_id();
-  const unsigned lt = (1u << lane) - 1u;
   const int64_t s = A.rp[row], e = A.rp[row + 1];
   int count = 0;
   for (int64_t base = s; base < e; base += 32) {
@@ -120,33 +202,21 @@ __device__ __forceinline__ int accumulate_row(const DCsr& A, const DCsr& B, int3
       len = (int)(RowOff<R32>::at(B, k + 1) - bs);
     }
     const int n = (int)min((int64_t)32, e - base);
-    for (int t = 0; t < n; ++t) {
-      const Off bst = __shfl_sync(kFull, bs, t);
-      const int l = __shfl_sync(kFull, len, t);
-      const float at = __shfl_sync(kFull, a, t);
-      for (int q0 = 0; q0 < l; q0 += 32) {
-        const int q = q0 + lane;
-        bool fresh = false, failed = false;
-        int32_t j = 0;
-        if (q < l) {
-          j = B.col[bst + q];
-          const float pr = prod_rn(at, B.val[bst + q]);
-          const int slot = table_insert(keys, LOGT, j, epoch, fresh);
-          if (slot < 0) failed = true;
-          else vals[slot] = add_rn(fresh ? 0.f : vals[slot], pr);
-        }
-        const unsigned m = __ballot_sync(kFull, fresh);
-        if (LEARNED) {
-          if (__any_sync(kFull, failed) || count + __popc(m) > cap) {
-            __syncwarp();
-            return -1;
-          }
-        } else if (failed) {
-          raise_flag(flags, kFlagHashFull);
-        }
-        if (fresh) list[count + __popc(m & lt)] = j;
-        count += __popc(m);
-        __syncwarp();
+    const unsigned long_mask = __ballot_sync(kFull, len >= kPackBelow);
+    int idx = 0;
+    while (idx < n) {
+      if ((long_mask >> idx) & 1u) {
+        const Off sbs = __shfl_sync(kFull, bs, idx);
+        const int sl = __shfl_sync(kFull, len, idx);
+        const float sa = __shfl_sync(kFull, a, idx);
+        if (!acc_segment<LOGT, LEARNED>(B, sbs, sl, sa, keys, vals, list, epoch, cap, count, flags)) return -1;
+        ++idx;
+      } else {
+        const unsigned later = long_mask & (~0u << idx);
+        const int hi = later ? min(n, __ffs(later) - 1) : n;
+        if (!acc_packed<LOGT, LEARNED>(B, bs, len, a, idx, hi, keys, vals, list, epoch, cap, count, flags))
+          return -1;
+        idx = hi;
       }
     }
   }
@@ -177,10 +247,107 @@ __device__ __forceinline__ void sort_lookup_write(const int32_t* keys, const flo
   }
 }
 
-// Writes the row's n entries in column order (register sort up to 512
-// entries, shared-memory bitonic sort of the list beyond that).
+// Writes the row's n entries in column order with a warp LSD radix sort.
+// Each listed column c becomes the word ((c - lo) << LOGT) | slot (lo = the
+// row's smallest column, slot = its table slot), so the sort carries the
+// value's location with it and no lookups follow.  Passes of `d`-bit digits
+// (d <= 8) cover the bits of the column span; each pass is a histogram, an
+// exclusive scan of the buckets and a stable scatter (32 words per step in
+// list order, ranks within a bucket from __match_any_sync).  Buffers: the
+// list and the key array take turns; the bucket counts live past the n
+// words of the source.  Returns false, touching nothing, when the packed
+// words do not fit 32 bits or the buffers are too small; on success the key
+// array is wiped (the caller's table is empty afterwards).
 template <int LOGT>
-__device__ __forceinline__ void emit_row(const int32_t* keys, const float* vals, int32_t* list, int n, int epoch,
+__device__ __forceinline__ bool radix_emit(int32_t* keys, const float* vals, int32_t* list, int n, int epoch,
+                                           int64_t limit, int32_t* out_col, float* out_val) {
+  constexpr int T = 1 << LOGT;
+  const int lane = lane_id();
+  const unsigned lt = (1u << lane) - 1u;
+  int lo = 0x7fffffff, hi = 0;
+  for (int i = lane; i < n; i += 32) {
+    const int c = list[i];
+    lo = min(lo, c);
+    hi = max(hi, c);
+  }
+  lo = (int)__reduce_min_sync(kFull, (unsigned)lo);
+  hi = (int)__reduce_max_sync(kFull, (unsigned)hi);
+  const uint32_t span = (uint32_t)(hi - lo);
+  const int span_bits = span ? 32 - __clz(span) : 0;
+  if (span_bits > 32 - LOGT) return false;
+  int d = 8;
+  while (d > 5 && n + (1 << d) > T) --d;
+  if (n + (1 << d) > T) return false;
+  // pack (reads the intact table)
+  for (int i = lane; i < n; i += 32) {
+    const int c = list[i];
+    const int slot = table_find(keys, LOGT, c, epoch);
+    list[i] = (int32_t)(((uint32_t)(c - lo) << LOGT) | (uint32_t)(slot & (T - 1)));
+  }
+  __syncwarp();
+  uint32_t* srcb = reinterpret_cast<uint32_t*>(list);
+  uint32_t* dstb = reinterpret_cast<uint32_t*>(keys);
+  const int nb = 1 << d;
+  const uint32_t dm = (uint32_t)nb - 1u;
+  for (int shift = LOGT; shift < LOGT + span_bits; shift += d) {
+    int* hist = reinterpret_cast<int*>(srcb + n);
+    for (int b = lane; b < nb; b += 32) hist[b] = 0;
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) atomicAdd(&hist[(srcb[i] >> shift) & dm], 1);
+    __syncwarp();
+    // exclusive scan of the buckets, nb / 32 (<= 8) consecutive per lane
+    const int per = (nb + 31) >> 5;
+    int loc[8];
+    int sum = 0;
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+      const int b = lane * per + x;
+      loc[x] = (x < per && b < nb) ? hist[b] : 0;
+      sum += loc[x];
+    }
+    int run = warp_incl_scan(sum) - sum;
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+      const int b = lane * per + x;
+      if (x < per && b < nb) hist[b] = run;
+      run += loc[x];
+    }
+    __syncwarp();
+    // stable scatter
+    for (int i0 = 0; i0 < n; i0 += 32) {
+      const int i = i0 + lane;
+      const bool act = i < n;
+      const uint32_t v = act ? srcb[i] : 0u;
+      const int dig = act ? (int)((v >> shift) & dm) : -1 - lane;
+      const unsigned grp = __match_any_sync(kFull, dig);
+      const int leader = __ffs(grp) - 1;
+      int base = 0;
+      if (act && lane == leader) base = atomicAdd(&hist[dig], __popc(grp));
+      base = __shfl_sync(kFull, base, leader);
+      if (act) dstb[base + __popc(grp & lt)] = v;
+    }
+    __syncwarp();
+    uint32_t* t = srcb;
+    srcb = dstb;
+    dstb = t;
+  }
+  const int m = (int)min((int64_t)n, limit);
+  for (int i = lane; i < m; i += 32) {
+    const uint32_t v = srcb[i];
+    out_col[i] = lo + (int32_t)(v >> LOGT);
+    out_val[i] = vals[v & (uint32_t)(T - 1)];
+  }
+  __syncwarp();
+  for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
+  __syncwarp();
+  return true;
+}
+
+// Writes the row's n entries in column order: register bitonic sorts up to
+// 128 entries, the radix sort above that, and (when the radix sort does not
+// apply) a register sort up to 256 entries or a shared-memory bitonic sort.
+template <int LOGT>
+__device__ __forceinline__ void emit_row(int32_t* keys, const float* vals, int32_t* list, int n, int epoch,
                                          int64_t limit, int32_t* out_col, float* out_val) {
   constexpr int T = 1 << LOGT;
   if (n <= 32) {
@@ -189,10 +356,10 @@ __device__ __forceinline__ void emit_row(const int32_t* keys, const float* vals,
     sort_lookup_write<2, LOGT>(keys, vals, list, n, epoch, limit, out_col, out_val);
   } else if (n <= 128) {
     sort_lookup_write<4, LOGT>(keys, vals, list, n, epoch, limit, out_col, out_val);
+  } else if (radix_emit<LOGT>(keys, vals, list, n, epoch, limit, out_col, out_val)) {
+    return;
   } else if (n <= 256) {
     sort_lookup_write<8, LOGT>(keys, vals, list, n, epoch, limit, out_col, out_val);
-  } else if (T >= 1024 && n <= 512) {
-    sort_lookup_write<16, LOGT>(keys, vals, list, n, epoch, limit, out_col, out_val);
   } else {
     const int lane = lane_id();
     warp_sort_keys(list, n, T);

@@ -156,6 +156,24 @@ spg_status spg_multiply(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_cs
                         const spg_opts* opts, spg_report* report);
 
 /*
+ * Value-only recompute: C already holds the structure of A * B (the result
+ * of an earlier spg_multiply on matrices with the same structure as A and
+ * B, on the device, either index width).  Recomputes C->val in place from
+ * the current values of A and B; the products pass, the symbolic pass and
+ * the scan are skipped (rows are binned by C's row lengths, heavy-row tiles
+ * are counted from C's sorted columns).  C->col_idx is rewritten with the
+ * same columns.  As with cuSPARSE's reuse, the caller guarantees that A and
+ * B keep the structure C was computed from; a differing count of distinct
+ * columns in a row (in a column tile holding entries of C, for rows beyond
+ * the warp tables) fails the call with SPG_ERR_INVALID_ARG.
+ * report->products is not computed (0).
+ * Replaces: cusparseSpGEMMreuse_compute after the structure phase
+ * (cuSparse/src/main.cpp:98-296, second compute with new values :286-296).
+ */
+spg_status spg_multiply_reuse(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_csr* C,
+                              const spg_opts* opts, spg_report* report);
+
+/*
  * n independent products C[i] = A[i] * B[i] of uneven sizes in one
  * persistent launch per stage that drains a device queue of
  * (matrix, row-bin) tiles; with opts->use_graph the launch sequence is

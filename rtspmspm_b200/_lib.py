@@ -104,6 +104,7 @@ SIGNATURES = [
     ("spg_set_stream", ctypes.c_int32, [_vp, _vp]),
     ("spg_get_stream", _vp, [_vp]),
     ("spg_multiply", ctypes.c_int32, [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
+    ("spg_multiply_reuse", ctypes.c_int32, [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
     ("spg_multiply_batched", ctypes.c_int32,
      [_vp, ctypes.c_int32, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
     ("spg_multiply_noalloc", ctypes.c_int32,

@@ -535,6 +535,52 @@ spg_status multiply_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, spg_c
   return check_flags(ctx, rep);
 }
 
+// Value-only recompute into an existing C (structure of A*B given).
+spg_status multiply_reuse_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, spg_csr* C, const spg_opts& o,
+                                 spg_report* rep) {
+  StageTimer tm(ctx, o.stage_timing != 0);
+  const spg_tuning t = o.use_tuning ? ctx->tuning : default_tuning();
+  Pipeline P(ctx, A, B, t);
+  SPG_TRY(P.init());
+  const LaunchCtx lc = P.lc;
+  const int64_t rows = P.rows;
+  tm.mark(SPG_STAGE_BINNING);
+  // C's row pointers as int64 (P.nnz), its row lengths as the numeric key
+  if (C->index_bits == 32) {
+    launch_widen_rp(static_cast<const int32_t*>(C->row_ptr), rows + 1, P.nnz.as<int64_t>(), lc);
+  } else {
+    SPG_CUDA(ctx, cudaMemcpyAsync(P.nnz.get(), C->row_ptr, (size_t)(rows + 1) * 8, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+  }
+  launch_row_lengths(P.nnz.as<int64_t>(), rows, P.prod.as<int64_t>(), lc);
+  ctx->launches += 2;
+  P.bin(P.prod.as<int64_t>(), kBinNumeric);
+  SPG_TRY(P.fetch_offsets());
+  const int64_t nheavy = P.bin_size(kBinHeavy);
+  if (nheavy > 0) {
+    const size_t tb = (size_t)nheavy * P.ntiles * 4;
+    SPG_TRY(P.tile_cnt.alloc(ctx, tb));
+    SPG_TRY(P.tile_off.alloc(ctx, tb));
+    SPG_CUDA(ctx, cudaMemsetAsync(P.tile_cnt.get(), 0, tb, ctx->stream));
+    launch_tile_counts_from_cols(P.bin_rows(kBinHeavy), nheavy, P.nnz.as<int64_t>(), C->col_idx, P.ntiles,
+                                 P.big_slot.as<int32_t>(), P.tile_cnt.as<int32_t>(), ctx->d_flags, lc);
+    ++ctx->launches;
+  }
+  tm.mark(SPG_STAGE_NUMERIC);
+  SPG_TRY(P.numeric(P.nnz.as<int64_t>(), C->col_idx, C->val, rep));
+  tm.finish(rep);
+  int f = 0;
+  SPG_TRY(read_flags(ctx, &f));
+  if (rep) {
+    rep->device_flags |= f;
+    rep->nnz_c = C->nnz;
+  }
+  if (f & kFlagCountDiff) return fail(ctx, SPG_ERR_INVALID_ARG, "the structure of C does not match A*B");
+  if (f & kFlagBadIndex) return fail(ctx, SPG_ERR_INVALID_ARG, "C has columns outside [0, cols)");
+  if (f & kFlagHashFull) return fail(ctx, SPG_ERR_INTERNAL, "device consistency check failed (flags %d)", f);
+  return SPG_OK;
+}
+
 spg_status row_nnz_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, int64_t* d_nnz) {
   Pipeline P(ctx, A, B, ctx->tuning);
   SPG_TRY(P.init());
@@ -674,6 +720,39 @@ spg_status spg_multiply(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_cs
     float ms = 0.f;
     (void)ms;
   }
+  return SPG_OK;
+}
+
+spg_status spg_multiply_reuse(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_csr* C, const spg_opts* opts,
+                              spg_report* report) {
+  if (!ctx) return SPG_ERR_INVALID_ARG;
+  if (!A || !B || !C) return fail(ctx, SPG_ERR_INVALID_ARG, "null argument");
+  if (A->cols != B->rows)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "inner dimensions differ (%lld vs %lld)", (long long)A->cols,
+                (long long)B->rows);
+  if (C->location != SPG_DEVICE) return fail(ctx, SPG_ERR_INVALID_ARG, "C must be on the device");
+  if (C->rows != A->rows || C->cols != B->cols)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "C is %lld x %lld, A*B is %lld x %lld", (long long)C->rows,
+                (long long)C->cols, (long long)A->rows, (long long)B->cols);
+  if (C->index_bits != 32 && C->index_bits != 64) return fail(ctx, SPG_ERR_INVALID_ARG, "bad C index_bits");
+  if (C->rows > 0 && !C->row_ptr) return fail(ctx, SPG_ERR_INVALID_ARG, "C has no row pointers");
+  if (C->nnz > 0 && (!C->col_idx || !C->val)) return fail(ctx, SPG_ERR_INVALID_ARG, "C has no column/value arrays");
+  if (A->rows > INT32_MAX) return fail(ctx, SPG_ERR_UNSUPPORTED, "more than 2^31-1 rows");
+  SPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  spg_opts o{};
+  if (opts) o = *opts;
+  if (report) {
+    std::memset(report, 0, sizeof *report);
+    report->algo = SPG_ALGO_PLAIN;
+    report->rows = A->rows;
+  }
+  const int launches0 = ctx->launches;
+  DevMat dA, dB;
+  SPG_TRY(prepare_matrix(ctx, A, dA, !o.skip_validation));
+  SPG_TRY(prepare_matrix(ctx, B, dB, !o.skip_validation));
+  if (!o.skip_validation) SPG_TRY(check_flags(ctx, report));
+  SPG_TRY(spg::multiply_reuse_device(ctx, dA, dB, C, o, report));
+  if (report) report->kernel_launches = ctx->launches - launches0;
   return SPG_OK;
 }
 

@@ -112,6 +112,9 @@ spg_status multiply_cusparse(spg_ctx* ctx, const DevMat& A, const DevMat& B, spg
                              spg_report* rep);
 // Exact per-row nnz of A*B (int64, rows entries) with the plain symbolic pass.
 spg_status row_nnz_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, int64_t* d_nnz);
+// Value-only recompute of C's values (C holds the structure of A*B).
+spg_status multiply_reuse_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, spg_csr* C, const spg_opts& o,
+                                 spg_report* rep);
 spg_status ensure_mlp(spg_ctx* ctx);
 void free_batch_cache(spg_ctx* ctx);
 

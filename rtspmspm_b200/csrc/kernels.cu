@@ -576,6 +576,62 @@ __global__ void k_build_blocked_index(DCsr B, int ntiles, int32_t* bidx) {
   }
 }
 
+// Value-only recompute (structure of C given): per-row lengths of C and,
+// for the rows of the heavy bin, their slot and per-tile entry counts taken
+// from C's sorted columns.
+
+// len[r] = rp[r + 1] - rp[r]
+__global__ void k_row_lengths(const int64_t* rp, int64_t rows, int64_t* len) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x)
+    len[r] = rp[r + 1] - rp[r];
+}
+
+// big_slot[heavy_rows[h]] = h; one warp per heavy row then counts the row's
+// entries per column tile (tile_cnt[h * ntiles + t], zeroed beforehand) from
+// the run starts of its sorted columns: a tile's count is the distance from
+// its first entry to the next tile's first entry (or the row end).
+__global__ void k_tile_counts_from_cols(const int32_t* heavy_rows, int64_t nheavy, const int64_t* c_rp,
+                                        const int32_t* c_col, int ntiles, int32_t* big_slot, int32_t* tile_cnt,
+                                        int* flags) {
+  const int lane = lane_id();
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t h = gw; h < nheavy; h += nw) {
+    const int32_t row = heavy_rows[h];
+    if (lane == 0) big_slot[row] = (int32_t)h;
+    int32_t* cnt = tile_cnt + h * ntiles;
+    const int64_t s = c_rp[row], e = c_rp[row + 1];
+    int pend_t = -1;     // tile whose run is still open (uniform)
+    int64_t pend_p = 0;  // its first entry
+    for (int64_t base = s; base < e; base += 32) {
+      const int64_t p = base + lane;
+      int t = -1;
+      bool first = false;
+      if (p < e) {
+        t = c_col[p] >> kTileShift;
+        first = p == s || (c_col[p - 1] >> kTileShift) != t;
+        if ((unsigned)t >= (unsigned)ntiles) {
+          raise_flag(flags, kFlagBadIndex);
+          first = false;
+        }
+      }
+      const unsigned fm = __ballot_sync(kFull, first);
+      if (fm) {
+        const int lead = __ffs(fm) - 1;
+        if (pend_t >= 0 && lane == 0) cnt[pend_t] = (int32_t)(base + lead - pend_p);
+        if (first) {
+          const unsigned later = fm & ~((2u << lane) - 1u);
+          if (later) cnt[t] = (int32_t)(__ffs(later) - 1 - lane);
+        }
+        const int last = 31 - __clz(fm);
+        pend_t = __shfl_sync(kFull, t, last);
+        pend_p = base + last;
+      }
+    }
+    if (pend_t >= 0 && lane == 0) cnt[pend_t] = (int32_t)(e - pend_p);
+  }
+}
+
 // Per heavy row: exclusive scan of its tile counts (warp per row slot).
 __global__ void k_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
                                const int32_t* tile_cnt, int ntiles, int32_t* tile_off) {
@@ -1110,6 +1166,19 @@ void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int3
     default: break;
   }
 #undef SPG_NWL
+}
+
+void launch_row_lengths(const int64_t* rp, int64_t rows, int64_t* len, const LaunchCtx& lc) {
+  if (rows == 0) return;
+  k_row_lengths<<<grid_for(rows, 256, 1, lc.sms * 8), 256, 0, lc.stream>>>(rp, rows, len);
+}
+
+void launch_tile_counts_from_cols(const int32_t* heavy_rows, int64_t nheavy, const int64_t* c_rp,
+                                  const int32_t* c_col, int ntiles, int32_t* big_slot, int32_t* tile_cnt, int* flags,
+                                  const LaunchCtx& lc) {
+  if (nheavy == 0) return;
+  k_tile_counts_from_cols<<<grid_for(nheavy, 256, 32, lc.sms * 8), 256, 0, lc.stream>>>(
+      heavy_rows, nheavy, c_rp, c_col, ntiles, big_slot, tile_cnt, flags);
 }
 
 void launch_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot, const int32_t* tile_cnt,

@@ -71,6 +71,12 @@ void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int3
                              const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
                              int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
                              const LaunchCtx& lc, int wpb);
+// Value-only recompute: row lengths of C, and heavy-row slots and per-tile
+// counts from C's sorted columns (tile_cnt zeroed by the caller).
+void launch_row_lengths(const int64_t* rp, int64_t rows, int64_t* len, const LaunchCtx& lc);
+void launch_tile_counts_from_cols(const int32_t* heavy_rows, int64_t nheavy, const int64_t* c_rp,
+                                  const int32_t* c_col, int ntiles, int32_t* big_slot, int32_t* tile_cnt, int* flags,
+                                  const LaunchCtx& lc);
 void launch_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot, const int32_t* tile_cnt,
                          int ntiles, int32_t* tile_off, const LaunchCtx& lc);
 void launch_build_blocked_index(const DCsr& B, int ntiles, int32_t* bidx, const LaunchCtx& lc);

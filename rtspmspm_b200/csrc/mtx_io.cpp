@@ -4,10 +4,12 @@
 // (cooFromFile cuSparse/src/util.cpp:9-44, mat1ToGPU
 // optixSpMSpM/src/optixSpMSpM/optixSpMSpM.cpp:73-131, Sphere::Sphere
 // optixSpMSpM/src/optixSpMSpM/Sphere.cpp:26-78).  The whole file is read
-// at once and parsed with std::from_chars; entries may come in any order
-// (the shipped fixtures are column-major), are converted to 0-based CSR with
-// sorted columns, and duplicate (i, j) pairs are summed in FP32 in file
-// order.  `symmetric` files are expanded; `pattern` files get value 1.
+// at once and its body parsed with std::from_chars in newline-aligned slices
+// on all host threads; entries may come in any order (the shipped fixtures
+// are column-major), are converted to 0-based CSR with sorted columns (row
+// blocks in parallel), and duplicate (i, j) pairs are summed in FP32 in file
+// order.  `symmetric` files are expanded; `pattern` files get value 1; lines
+// after the header's nnz entries are ignored.
 //
 // Writer: the reference's two writers -- printCooToFile
 // (cuSparse/src/util.cpp:49-69, every structural entry) and printResult
@@ -22,6 +24,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -91,8 +94,69 @@ std::string lower(std::string s) {
   return s;
 }
 
+// Entries of one newline-aligned slice of the body, in file order.
+struct Slice {
+  std::vector<int32_t> ri, ci;
+  std::vector<float> vv;
+  int64_t entries = 0;  // file entries (before symmetric expansion)
+  bool bad = false;
+};
+
+void parse_slice(const char* b, const char* e, bool pattern, bool symmetric, bool skew, int64_t rows, int64_t cols,
+                 Slice& out) {
+  Cursor c{b, e};
+  while (!c.at_end()) {
+    c.skip_blank();
+    if (c.at_end()) break;
+    if (*c.p == '\n' || *c.p == '%') {
+      c.next_line();
+      continue;
+    }
+    int64_t i = 0, j = 0;
+    float v = 1.0f;
+    if (!c.read_int(i) || !c.read_int(j) || (!pattern && !c.read_float(v)) || i < 1 || i > rows || j < 1 ||
+        j > cols) {
+      out.bad = true;
+      return;
+    }
+    out.ri.push_back((int32_t)(i - 1));
+    out.ci.push_back((int32_t)(j - 1));
+    out.vv.push_back(v);
+    if (symmetric && i != j) {
+      out.ri.push_back((int32_t)(j - 1));
+      out.ci.push_back((int32_t)(i - 1));
+      out.vv.push_back(skew ? -v : v);
+    }
+    ++out.entries;
+    c.next_line();
+  }
+}
+
+int worker_count(size_t work, size_t per_worker) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t want = std::max<size_t>(1, work / std::max<size_t>(per_worker, 1));
+  return (int)std::min<size_t>({(size_t)hw, want, (size_t)64});
+}
+
+template <typename F>
+void run_workers(int n, F&& f) {
+  if (n <= 1) {
+    f(0);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve((size_t)n - 1);
+  for (int t = 1; t < n; ++t) th.emplace_back(f, t);
+  f(0);
+  for (auto& x : th) x.join();
+}
+
 }  // namespace
 
+// Parses the body in newline-aligned slices on all host threads, then builds
+// CSR: a counting sort by row keeps file order inside a row, and row blocks
+// (balanced by entries) are sorted by column and their duplicates summed in
+// file order in parallel.
 extern "C" spg_status spg_mtx_read(const char* path, spg_csr* out) {
   if (!path || !out) return SPG_ERR_INVALID_ARG;
   std::memset(out, 0, sizeof *out);
@@ -125,78 +189,106 @@ extern "C" spg_status spg_mtx_read(const char* path, spg_csr* out) {
   if (!c.read_int(rows) || !c.read_int(cols) || !c.read_int(nnz)) return SPG_ERR_FORMAT;
   if (rows < 0 || cols < 0 || nnz < 0 || cols > INT32_MAX || rows > INT32_MAX) return SPG_ERR_FORMAT;
   c.next_line();
-  const int64_t cap = symmetric ? 2 * nnz : nnz;
-  std::vector<int32_t> ri, ci;
-  std::vector<float> vv;
-  ri.reserve((size_t)cap);
-  ci.reserve((size_t)cap);
-  vv.reserve((size_t)cap);
-  int64_t seen = 0;
-  while (seen < nnz) {
-    c.skip_blank();
-    if (c.at_end()) return SPG_ERR_FORMAT;
-    if (*c.p == '\n' || *c.p == '%') {
-      c.next_line();
-      continue;
-    }
-    int64_t i = 0, j = 0;
-    float v = 1.0f;
-    if (!c.read_int(i) || !c.read_int(j)) return SPG_ERR_FORMAT;
-    if (!pattern && !c.read_float(v)) return SPG_ERR_FORMAT;
-    if (i < 1 || i > rows || j < 1 || j > cols) return SPG_ERR_FORMAT;
-    ri.push_back((int32_t)(i - 1));
-    ci.push_back((int32_t)(j - 1));
-    vv.push_back(v);
-    if (symmetric && i != j) {
-      ri.push_back((int32_t)(j - 1));
-      ci.push_back((int32_t)(i - 1));
-      vv.push_back(skew ? -v : v);
-    }
-    ++seen;
-    c.next_line();
+  // ---- parse: slices cut at line starts ----
+  const char* body = c.p;
+  const size_t blen = (size_t)(c.end - body);
+  const int ns = worker_count(blen, (size_t)4 << 20);
+  std::vector<const char*> cut((size_t)ns + 1);
+  cut[0] = body;
+  cut[(size_t)ns] = c.end;
+  for (int t = 1; t < ns; ++t) {
+    const char* q = body + blen * (size_t)t / (size_t)ns;
+    if (q < cut[(size_t)t - 1]) q = cut[(size_t)t - 1];
+    while (q < c.end && q[-1] != '\n') ++q;
+    cut[(size_t)t] = q;
   }
-  // counting sort by row (stable: keeps file order inside a row)
-  const size_t m = ri.size();
+  std::vector<Slice> sl((size_t)ns);
+  run_workers(ns, [&](int t) {
+    parse_slice(cut[(size_t)t], cut[(size_t)t + 1], pattern, symmetric, skew, rows, cols, sl[(size_t)t]);
+  });
+  // the first nnz entries count (later lines are ignored); a malformed line
+  // before them is an error
+  int64_t seen = 0, m = 0;
+  int last = -1;
+  for (int t = 0; t < ns && seen < nnz; ++t) {
+    if (sl[(size_t)t].bad && seen + sl[(size_t)t].entries < nnz) return SPG_ERR_FORMAT;
+    last = t;
+    if (seen + sl[(size_t)t].entries > nnz) {
+      // trim this slice to the entries still wanted (expanded pairs stay together)
+      Slice& z = sl[(size_t)t];
+      const int64_t keep = nnz - seen;
+      size_t k = 0;
+      for (int64_t x = 0; x < keep; ++x) k += (symmetric && z.ri[k] != z.ci[k]) ? 2 : 1;
+      z.ri.resize(k);
+      z.ci.resize(k);
+      z.vv.resize(k);
+      z.entries = keep;
+    }
+    seen += sl[(size_t)t].entries;
+    m += (int64_t)sl[(size_t)t].ri.size();
+  }
+  if (seen < nnz) return SPG_ERR_FORMAT;
+  // ---- counting sort by row (stable: file order inside a row) ----
   std::vector<int64_t> rp((size_t)rows + 1, 0);
-  for (size_t t = 0; t < m; ++t) ++rp[(size_t)ri[t] + 1];
+  for (int t = 0; t <= last; ++t)
+    for (int32_t r : sl[(size_t)t].ri) ++rp[(size_t)r + 1];
   for (int64_t r = 0; r < rows; ++r) rp[(size_t)r + 1] += rp[(size_t)r];
-  std::vector<int64_t> pos(rp.begin(), rp.end() - 1);
-  std::vector<int32_t> col(m);
-  std::vector<float> val(m);
-  for (size_t t = 0; t < m; ++t) {
-    const int64_t d = pos[(size_t)ri[t]]++;
-    col[(size_t)d] = ci[t];
-    val[(size_t)d] = vv[t];
-  }
-  ri.clear();
-  ri.shrink_to_fit();
-  ci.clear();
-  ci.shrink_to_fit();
-  vv.clear();
-  vv.shrink_to_fit();
-  // sort columns per row (stable), merge duplicates in file order
-  std::vector<int64_t> orp((size_t)rows + 1, 0);
-  std::vector<std::pair<int32_t, float>> tmp;
-  int64_t w = 0;
-  for (int64_t r = 0; r < rows; ++r) {
-    const int64_t s = rp[(size_t)r], e = rp[(size_t)r + 1];
-    tmp.assign(e - s, {});
-    for (int64_t t = s; t < e; ++t) tmp[(size_t)(t - s)] = {col[(size_t)t], val[(size_t)t]};
-    std::stable_sort(tmp.begin(), tmp.end(),
-                     [](const std::pair<int32_t, float>& a, const std::pair<int32_t, float>& b) {
-                       return a.first < b.first;
-                     });
-    for (size_t t = 0; t < tmp.size(); ++t) {
-      if (t > 0 && tmp[t].first == tmp[t - 1].first) {
-        val[(size_t)(w - 1)] = val[(size_t)(w - 1)] + tmp[t].second;
-      } else {
-        col[(size_t)w] = tmp[t].first;
-        val[(size_t)w] = tmp[t].second;
-        ++w;
+  std::vector<int32_t> col((size_t)m);
+  std::vector<float> val((size_t)m);
+  {
+    std::vector<int64_t> pos(rp.begin(), rp.end() - 1);
+    for (int t = 0; t <= last; ++t) {
+      Slice& z = sl[(size_t)t];
+      for (size_t k = 0; k < z.ri.size(); ++k) {
+        const int64_t d = pos[(size_t)z.ri[k]]++;
+        col[(size_t)d] = z.ci[k];
+        val[(size_t)d] = z.vv[k];
       }
+      z = Slice();
     }
-    orp[(size_t)r + 1] = w;
   }
+  // ---- per-row column sort + duplicate merge, row blocks in parallel ----
+  const int nb = worker_count((size_t)m, (size_t)1 << 20);
+  std::vector<int64_t> r0((size_t)nb + 1, rows);
+  r0[0] = 0;
+  for (int t = 1; t < nb; ++t) {
+    const int64_t target = m * t / nb;
+    r0[(size_t)t] = std::upper_bound(rp.begin(), rp.end(), target) - rp.begin() - 1;
+    if (r0[(size_t)t] < r0[(size_t)t - 1]) r0[(size_t)t] = r0[(size_t)t - 1];
+  }
+  std::vector<int64_t> rowlen((size_t)rows, 0);
+  run_workers(nb, [&](int t) {
+    std::vector<std::pair<int32_t, float>> tmp;
+    for (int64_t r = r0[(size_t)t]; r < r0[(size_t)t + 1]; ++r) {
+      const int64_t s = rp[(size_t)r], e = rp[(size_t)r + 1];
+      bool sorted = true;
+      for (int64_t q = s + 1; q < e && sorted; ++q) sorted = col[(size_t)q - 1] < col[(size_t)q];
+      if (sorted) {
+        rowlen[(size_t)r] = e - s;
+        continue;
+      }
+      tmp.assign((size_t)(e - s), {});
+      for (int64_t q = s; q < e; ++q) tmp[(size_t)(q - s)] = {col[(size_t)q], val[(size_t)q]};
+      std::stable_sort(tmp.begin(), tmp.end(),
+                       [](const std::pair<int32_t, float>& x, const std::pair<int32_t, float>& y) {
+                         return x.first < y.first;
+                       });
+      int64_t w = s;
+      for (size_t q = 0; q < tmp.size(); ++q) {
+        if (q > 0 && tmp[q].first == tmp[q - 1].first) {
+          val[(size_t)w - 1] = val[(size_t)w - 1] + tmp[q].second;
+        } else {
+          col[(size_t)w] = tmp[q].first;
+          val[(size_t)w] = tmp[q].second;
+          ++w;
+        }
+      }
+      rowlen[(size_t)r] = w - s;
+    }
+  });
+  std::vector<int64_t> orp((size_t)rows + 1, 0);
+  for (int64_t r = 0; r < rows; ++r) orp[(size_t)r + 1] = orp[(size_t)r] + rowlen[(size_t)r];
+  const int64_t w = orp[(size_t)rows];
   const size_t rpb = ((size_t)rows + 1) * sizeof(int64_t);
   int64_t* hrp = (int64_t*)std::malloc(rpb);
   int32_t* hcol = (int32_t*)std::malloc(std::max<size_t>((size_t)w * 4, 4));
@@ -208,10 +300,14 @@ extern "C" spg_status spg_mtx_read(const char* path, spg_csr* out) {
     return SPG_ERR_OUT_OF_MEMORY;
   }
   std::memcpy(hrp, orp.data(), rpb);
-  if (w) {
-    std::memcpy(hcol, col.data(), (size_t)w * 4);
-    std::memcpy(hval, val.data(), (size_t)w * 4);
-  }
+  run_workers(nb, [&](int t) {
+    for (int64_t r = r0[(size_t)t]; r < r0[(size_t)t + 1]; ++r) {
+      const int64_t n = rowlen[(size_t)r];
+      if (!n) continue;
+      std::memcpy(hcol + orp[(size_t)r], col.data() + rp[(size_t)r], (size_t)n * 4);
+      std::memcpy(hval + orp[(size_t)r], val.data() + rp[(size_t)r], (size_t)n * 4);
+    }
+  });
   out->rows = rows;
   out->cols = cols;
   out->nnz = w;

@@ -237,6 +237,23 @@ class Engine:
                                         ctypes.byref(o), ctypes.byref(rep)))
         return Result(self, c), rep.as_dict()
 
+    def multiply_reuse(self, A, B, C: "Result", **kw):
+        """Recomputes the values of C = A*B in place; C (a device Result of an
+        earlier multiply) holds the structure of A*B. Returns the report dict."""
+        sa, ka = self._as_struct(A, self.device)
+        sb, kb = self._as_struct(B, self.device)
+        o = self.opts(**kw)
+        rep = _lib.SpgReport()
+        self._check(self.L.spg_multiply_reuse(self.ctx, ctypes.byref(sa), ctypes.byref(sb), ctypes.byref(C.s),
+                                              ctypes.byref(o), ctypes.byref(rep)))
+        return rep.as_dict()
+
+    def multiply_reuse_raw(self, sa: _lib.SpgCsr, sb: _lib.SpgCsr, o: _lib.SpgOpts, c: _lib.SpgCsr,
+                           rep: _lib.SpgReport) -> None:
+        """Low-overhead value-only recompute on prepared structs (benchmark loops)."""
+        self._check(self.L.spg_multiply_reuse(self.ctx, ctypes.byref(sa), ctypes.byref(sb), ctypes.byref(c),
+                                              ctypes.byref(o), ctypes.byref(rep)))
+
     def multiply_raw(self, sa: _lib.SpgCsr, sb: _lib.SpgCsr, o: _lib.SpgOpts, c: _lib.SpgCsr,
                      rep: _lib.SpgReport) -> None:
         """Low-overhead call on prepared structs (benchmark loops)."""

@@ -145,3 +145,54 @@ def test_drop_zeros_writer(tmp_path):
     assert lines[1] == "2 3 1" and lines[2] == "1 3 1"
     write_mtx(p, m)
     assert open(p).read().split("\n")[1] == "2 3 3"
+
+
+def _lines(r, c, v):
+    return "".join(f"{i + 1} {j + 1} {x:g}\n" for i, j, x in zip(r, c, v))
+
+
+def test_large_shuffled_file_parsed_in_slices(tmp_path):
+    """A body of several MB is parsed in newline-aligned slices on all host
+    threads: shuffled order, duplicates summed in file order, comment and
+    blank lines inside the body, extra lines past the header's count."""
+    rng = np.random.default_rng(5)
+    n, m = 3000, 900_000
+    r = rng.integers(0, n, m)
+    c = rng.integers(0, n, m)
+    v = rng.integers(-8, 9, m).astype(np.float32)  # small integers: every FP32 sum is exact
+    body = _lines(r, c, v)
+    cut = len(body) // 2
+    cut = body.index("\n", cut) + 1
+    text = ("%%MatrixMarket matrix coordinate real general\n% head comment\n"
+            f"{n} {n} {m}\n" + body[:cut] + "% mid comment\n\n" + body[cut:] + "1 1 99\n2 2 99\n")
+    p = tmp_path / "big.mtx"
+    p.write_text(text)
+    assert p.stat().st_size > 2 * (4 << 20)  # at least two 4 MB slices
+    got = read_mtx(str(p))
+    want = coo_to_csr(n, n, r, c, v, merge="sum")
+    np.testing.assert_array_equal(got.row_ptr, want.row_ptr)
+    np.testing.assert_array_equal(got.col_idx, want.col_idx)
+    np.testing.assert_array_equal(got.val, want.val)
+
+
+def test_symmetric_file_in_slices_and_truncated_body(tmp_path):
+    rng = np.random.default_rng(6)
+    n, m = 2000, 400_000
+    r = rng.integers(0, n, m)
+    c = rng.integers(0, n, m)
+    lo, hi = np.minimum(r, c), np.maximum(r, c)
+    v = rng.integers(1, 5, m).astype(np.float32)
+    p = tmp_path / "sym.mtx"
+    p.write_text(f"%%MatrixMarket matrix coordinate real symmetric\n{n} {n} {m}\n" + _lines(hi, lo, v))
+    got = read_mtx(str(p))
+    off = hi != lo
+    want = coo_to_csr(n, n, np.concatenate([hi, lo[off]]), np.concatenate([lo, hi[off]]),
+                      np.concatenate([v, v[off]]), merge="sum")
+    np.testing.assert_array_equal(got.row_ptr, want.row_ptr)
+    np.testing.assert_array_equal(got.col_idx, want.col_idx)
+    np.testing.assert_array_equal(got.val, want.val)
+    # a header promising more entries than the body holds is an error
+    p.write_text(f"%%MatrixMarket matrix coordinate real symmetric\n{n} {n} {m + 1}\n" + _lines(hi, lo, v))
+    with pytest.raises(SpgError) as e:
+        read_mtx(str(p))
+    assert e.value.status == 5

@@ -230,6 +230,15 @@ spg_status spg_csr_download(spg_ctx* ctx, const spg_csr* src, void* row_ptr, int
  */
 spg_status spg_csr_extract_rows(spg_ctx* ctx, const spg_csr* src, const int64_t* rows, int64_t n, spg_csr* dst);
 
+/*
+ * Transpose of a host matrix into a new host matrix (int64 row pointers,
+ * library-owned; release with spg_csr_free): a counting sort by column that
+ * visits rows in order, so every row of the transpose keeps ascending
+ * columns.  For C = A * B^T inputs, which the reference harness leaves as a
+ * TODO (scripts/AE_test.py:165-171, 216-217).
+ */
+spg_status spg_csr_transpose(const spg_csr* src, spg_csr* dst);
+
 /* ---- Matrix Market IO (host) --------------------------------------------- */
 
 /*
@@ -318,7 +327,10 @@ typedef struct spg_tuning {
     float   predict_margin;    /* learned: capacity = margin * predicted + slack */
     int32_t predict_slack;
     float   learned_load;      /* learned: table load factor at the predicted capacity */
-    int32_t reserved[4];
+    int32_t heavy_path;        /* rows beyond the warp tables: 0 = every column tile rescans
+                                  its row of A; 1 = products staged once per tile in HBM
+                                  buckets when they fit (else as 0) */
+    int32_t reserved[3];
 } spg_tuning;
 
 spg_status spg_get_tuning(spg_ctx* ctx, spg_tuning* out);

@@ -5,7 +5,8 @@ ABI of include/rtspmspm.h); this package is the host-side binding, the
 synthetic workload generators and the build script.
 """
 from . import gen
-from .engine import DeviceCsr, Engine, HostCsr, Result, SpgError, read_mtx, write_mtx
+from .engine import DeviceCsr, Engine, HostCsr, Result, SpgError, read_mtx, transpose, write_mtx
 from .gen import Csr
 
-__all__ = ["gen", "Csr", "DeviceCsr", "Engine", "HostCsr", "Result", "SpgError", "read_mtx", "write_mtx"]
+__all__ = ["gen", "Csr", "DeviceCsr", "Engine", "HostCsr", "Result", "SpgError", "read_mtx", "transpose",
+           "write_mtx"]

@@ -86,7 +86,7 @@ class SpgTuning(ctypes.Structure):
                 ("max_load", ctypes.c_float), ("tile_cols", ctypes.c_int32),
                 ("block_table_max", ctypes.c_int32), ("predict_margin", ctypes.c_float),
                 ("predict_slack", ctypes.c_int32), ("learned_load", ctypes.c_float),
-                ("reserved", ctypes.c_int32 * 4)]
+                ("heavy_path", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
@@ -104,6 +104,7 @@ SIGNATURES = [
     ("spg_set_stream", ctypes.c_int32, [_vp, _vp]),
     ("spg_get_stream", _vp, [_vp]),
     ("spg_multiply", ctypes.c_int32, [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
+    ("spg_csr_transpose", ctypes.c_int32, [_P(SpgCsr), _P(SpgCsr)]),
     ("spg_multiply_reuse", ctypes.c_int32, [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
     ("spg_multiply_batched", ctypes.c_int32,
      [_vp, ctypes.c_int32, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),

@@ -320,21 +320,32 @@ struct Pipeline {
     if (nheavy > 0) {
       launch_tile_offsets(bin_rows(kBinHeavy), nheavy, big_slot.as<int32_t>(), tile_cnt.as<int32_t>(), ntiles,
                           tile_off.as<int32_t>(), lc);
-      // blocked index of B when it fits the budget (else per-tile binary searches)
-      DevBuf bidx;
-      const size_t bidx_bytes = (size_t)B.view.rows * (size_t)(ntiles + 1) * 4;
-      size_t free_b = 0, total_b = 0;
-      cudaMemGetInfo(&free_b, &total_b);
-      const bool use_index = ntiles > 1 && bidx_bytes <= kBlockedIndexMaxBytes && bidx_bytes < free_b / 4;
-      if (use_index) {
-        SPG_TRY(bidx.alloc(ctx, bidx_bytes));
-        launch_build_blocked_index(B.view, ntiles, bidx.as<int32_t>(), lc);
-        ++ctx->launches;
+      // staged path (opt-in): each heavy row's products walked once into
+      // per-tile buckets; measured slower than rescanning on R-MAT (the
+      // bucket writes scatter over a buffer far larger than L2)
+      bool staged = false;
+      if (tune.heavy_path == 1)
+        SPG_TRY(heavy_staged(ctx, A.view, B.view, bin_rows(kBinHeavy), nheavy, big_slot.as<int32_t>(),
+                             tile_cnt.as<int32_t>(), tile_off.as<int32_t>(), ntiles, c_rp, c_col, c_val, &staged));
+      if (!staged) {
+        // rescanning tile kernel, with a blocked index of B when it fits the
+        // budget (else per-tile binary searches)
+        DevBuf bidx;
+        const size_t bidx_bytes = (size_t)B.view.rows * (size_t)(ntiles + 1) * 4;
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const bool use_index = ntiles > 1 && bidx_bytes <= kBlockedIndexMaxBytes && bidx_bytes < free_b / 4;
+        if (use_index) {
+          SPG_TRY(bidx.alloc(ctx, bidx_bytes));
+          launch_build_blocked_index(B.view, ntiles, bidx.as<int32_t>(), lc);
+          ++ctx->launches;
+        }
+        launch_num_tile(A.view, B.view, bin_rows(kBinHeavy), nheavy, big_slot.as<int32_t>(),
+                        tile_cnt.as<int32_t>(), tile_off.as<int32_t>(), ntiles, c_rp, c_col, c_val,
+                        use_index ? bidx.as<int32_t>() : nullptr, ctx->d_counter, ctx->d_flags, lc);
+        ctx->launches += 2;
       }
-      launch_num_tile(A.view, B.view, bin_rows(kBinHeavy), nheavy, big_slot.as<int32_t>(), tile_cnt.as<int32_t>(),
-                      tile_off.as<int32_t>(), ntiles, c_rp, c_col, c_val, use_index ? bidx.as<int32_t>() : nullptr,
-                      ctx->d_counter, ctx->d_flags, lc);
-      ctx->launches += 3;
+      ++ctx->launches;
     }
     if (rep) {
       for (int b = 0; b < kNumBins && b < SPG_NUM_BINS; ++b) rep->bin_rows[b] += bin_size(b);

@@ -321,6 +321,9 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
   p->n = n;
   p->key = plan_key(ctx, n, A, B, o);
   p->tune = o.use_tuning ? ctx->tuning : default_tuning();
+  // every warp table size stays available on the persistent path: a smaller
+  // tuned maximum would send whole products to the one-by-one path
+  p->tune.warp_table_max = default_tuning().warp_table_max;
   const BinParams bp = bin_params(p->tune);
   const LaunchCtx lc = launch_ctx(ctx);
   p->mats.resize((size_t)n);

@@ -12,7 +12,9 @@
 // 1 on any failure (optixSpMSpM.cpp:654-659).
 // Extra flags: --algo plain|learned|cusparse, --json report.json,
 // --tune-cache tune.json, --drop-zeros (skip exact zeros like the
-// ray-tracing writer), --device N, --mlp weights.bin.
+// ray-tracing writer), --device N, --mlp weights.bin, --transpose-m2 (C =
+// A * B^T for rectangular inputs; the reference harness leaves these as a
+// TODO, scripts/AE_test.py:165-171).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -35,6 +37,7 @@ void usage(const char* argv0) {
                "         --tune-cache <filename>     Autotune (cached per shape class and GPU)\n"
                "         --mlp <filename>            Predictor weights for --algo learned\n"
                "         --drop-zeros                Skip entries whose value is exactly 0\n"
+               "         --transpose-m2              Multiply by the transpose of matrix 2\n"
                "         --device <n>\n"
                "         --help | -h                 Print this usage message\n",
                argv0);
@@ -50,7 +53,7 @@ int die(spg_ctx* ctx, const char* what, spg_status st) {
 
 int main(int argc, char** argv) {
   std::string m1, m2, out, log, json, tune_cache, mlp;
-  int algo = SPG_ALGO_LEARNED, device = 0, drop_zeros = 0;
+  int algo = SPG_ALGO_LEARNED, device = 0, drop_zeros = 0, transpose_b = 0;
   for (int i = 1; i < argc; ++i) {
     const std::string a(argv[i]);
     auto next = [&]() -> std::string {
@@ -66,6 +69,7 @@ int main(int argc, char** argv) {
     else if (a == "--tune-cache") tune_cache = next();
     else if (a == "--mlp") mlp = next();
     else if (a == "--drop-zeros") drop_zeros = 1;
+    else if (a == "--transpose-m2") transpose_b = 1;
     else if (a == "--device") device = std::atoi(next().c_str());
     else if (a == "--algo") {
       const std::string v = next();
@@ -85,6 +89,12 @@ int main(int argc, char** argv) {
   if (st != SPG_OK) return die(nullptr, ("reading " + m1).c_str(), st);
   st = spg_mtx_read(m2.c_str(), &B);
   if (st != SPG_OK) return die(nullptr, ("reading " + m2).c_str(), st);
+  if (transpose_b) {
+    spg_csr T{};
+    if ((st = spg_csr_transpose(&B, &T)) != SPG_OK) return die(nullptr, "transposing -m2", st);
+    spg_csr_free(nullptr, &B);
+    B = T;
+  }
   if (A.cols != B.rows) {
     std::fprintf(stderr, "spgemm: inner dimensions differ (%lld vs %lld)\n", (long long)A.cols, (long long)B.rows);
     return 1;

@@ -112,6 +112,12 @@ spg_status multiply_cusparse(spg_ctx* ctx, const DevMat& A, const DevMat& B, spg
                              spg_report* rep);
 // Exact per-row nnz of A*B (int64, rows entries) with the plain symbolic pass.
 spg_status row_nnz_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, int64_t* d_nnz);
+// Heavy-row numeric pass through per-tile staging buckets (heavy.cu);
+// *done = false (nothing launched) when it does not apply.
+spg_status heavy_staged(spg_ctx* ctx, const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy,
+                        const int32_t* big_slot, const int32_t* tile_cnt, const int32_t* tile_off, int ntiles,
+                        const int64_t* c_rp, int32_t* c_col, float* c_val, bool* done);
+
 // Value-only recompute of C's values (C holds the structure of A*B).
 spg_status multiply_reuse_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, spg_csr* C, const spg_opts& o,
                                  spg_report* rep);

@@ -15,6 +15,7 @@
 //       (optixSpMSpM.cpp:452-494), done per row on the device.
 #include "common.cuh"
 #include "kernels.hpp"
+#include "tile.cuh"
 #include "warp_row.cuh"
 
 namespace spg {
@@ -751,21 +752,6 @@ __device__ __forceinline__ void tile_packed(const DCsr& B, Off bs, int len, floa
   }
 }
 
-// Position of the r-th (0-based) set bit of w; requires r < popc(w).
-__device__ __forceinline__ int nth_set_bit(uint32_t w, int r) {
-  int pos = 0;
-#pragma unroll
-  for (int s = 16; s > 0; s >>= 1) {
-    const int c = __popc(w & ((1u << s) - 1u));
-    if (r >= c) {
-      r -= c;
-      w >>= s;
-      pos += s;
-    }
-  }
-  return pos;
-}
-
 // One warp per (heavy row, 2^kTileShift-column tile), tiles handed out by an atomic
 // ticket.  A's row is read 32 entries at a time (the next 32 loaded while the
 // current ones are processed); each entry's B row is narrowed to the tile
@@ -783,7 +769,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
   using Off = typename RowOff<R32>::T;
   extern __shared__ uint32_t sm_tile[];
   const int lane = lane_id(), wib = threadIdx.x >> 5;
-  float* acc = reinterpret_cast<float*>(sm_tile) + (size_t)wib * (kTileCols + kTileWords + 32);
+  float* acc = reinterpret_cast<float*>(sm_tile) + (size_t)wib * kTileWarpWords;
   uint32_t* bits = reinterpret_cast<uint32_t*>(acc + kTileCols);
   float* stage = reinterpret_cast<float*>(bits + kTileWords);
   for (int s = lane; s < kTileCols; s += 32) acc[s] = 0.f;
@@ -856,39 +842,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
         }
       }
     }
-    // emit in column order, 32 words (1024 columns) per round; lanes take
-    // consecutive entries, so the stores are coalesced
-    int64_t pos = out;
-    const int64_t lim = out + want;
-    int found = 0;
-#pragma unroll 1
-    for (int g = 0; g < kTileWords; g += 32) {
-      const uint32_t wd = bits[g + lane];
-      const int c = __popc(wd);
-      const int inc = warp_incl_scan(c);
-      const int tot = __shfl_sync(kFull, inc, 31);
-      const int exc = inc - c;
-      for (int e0 = 0; e0 < tot; e0 += 32) {
-        const int ei = e0 + lane;
-        const bool act = ei < tot;
-        const int src = warp_upper_bound(inc, act ? ei : tot - 1);
-        const uint32_t sw = __shfl_sync(kFull, wd, src);
-        const int sex = __shfl_sync(kFull, exc, src);
-        if (act) {
-          const int off = ((g + src) << 5) + nth_set_bit(sw, ei - sex);
-          if (pos + ei < lim) {
-            c_col[pos + ei] = c0 + off;
-            c_val[pos + ei] = acc[off];
-          }
-          acc[off] = 0.f;
-        }
-      }
-      bits[g + lane] = 0u;
-      pos += tot;
-      found += tot;
-    }
-    if (found != want && lane == 0) raise_flag(flags, kFlagCountDiff);
-    __syncwarp();
+    tile_emit(acc, bits, c0, out, want, c_col, c_val, flags);
   }
 }
 

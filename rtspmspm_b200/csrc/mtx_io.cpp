@@ -321,6 +321,58 @@ extern "C" spg_status spg_mtx_read(const char* path, spg_csr* out) {
   return SPG_OK;
 }
 
+extern "C" spg_status spg_csr_transpose(const spg_csr* src, spg_csr* dst) {
+  if (!src || !dst || src == dst) return SPG_ERR_INVALID_ARG;
+  if (src->location != SPG_HOST) return SPG_ERR_INVALID_ARG;
+  if (src->index_bits != 32 && src->index_bits != 64) return SPG_ERR_INVALID_ARG;
+  if (src->rows > INT32_MAX || src->cols > INT32_MAX || src->nnz < 0) return SPG_ERR_UNSUPPORTED;
+  auto rp_at = [&](int64_t r) -> int64_t {
+    return src->index_bits == 64 ? static_cast<const int64_t*>(src->row_ptr)[r]
+                                 : (int64_t) static_cast<const int32_t*>(src->row_ptr)[r];
+  };
+  const int64_t rows = src->rows, cols = src->cols, nnz = src->nnz;
+  int64_t* trp = (int64_t*)std::calloc((size_t)cols + 1, sizeof(int64_t));
+  int32_t* tcol = (int32_t*)std::malloc(std::max<size_t>((size_t)nnz * 4, 4));
+  float* tval = (float*)std::malloc(std::max<size_t>((size_t)nnz * 4, 4));
+  if (!trp || !tcol || !tval) {
+    std::free(trp);
+    std::free(tcol);
+    std::free(tval);
+    return SPG_ERR_OUT_OF_MEMORY;
+  }
+  for (int64_t t = 0; t < nnz; ++t) {
+    const int32_t j = src->col_idx[t];
+    if (j < 0 || j >= cols) {
+      std::free(trp);
+      std::free(tcol);
+      std::free(tval);
+      return SPG_ERR_INVALID_ARG;
+    }
+    ++trp[(size_t)j + 1];
+  }
+  for (int64_t j = 0; j < cols; ++j) trp[j + 1] += trp[j];
+  std::vector<int64_t> pos(trp, trp + cols);
+  for (int64_t r = 0; r < rows; ++r) {
+    for (int64_t t = rp_at(r), e = rp_at(r + 1); t < e; ++t) {
+      const int64_t d = pos[(size_t)src->col_idx[t]]++;
+      tcol[d] = (int32_t)r;
+      tval[d] = src->val[t];
+    }
+  }
+  std::memset(dst, 0, sizeof *dst);
+  dst->rows = cols;
+  dst->cols = rows;
+  dst->nnz = nnz;
+  dst->capacity = nnz;
+  dst->index_bits = 64;
+  dst->location = SPG_HOST;
+  dst->row_ptr = trp;
+  dst->col_idx = tcol;
+  dst->val = tval;
+  dst->owner = 2;
+  return SPG_OK;
+}
+
 extern "C" spg_status spg_mtx_write(spg_ctx* ctx, const char* path, const spg_csr* m, int32_t drop_zeros) {
   if (!path || !m) return SPG_ERR_INVALID_ARG;
   spg_csr host{};

@@ -130,6 +130,7 @@ spg_status spg_set_tuning(spg_ctx* ctx, const spg_tuning* in) {
   if (t.predict_margin <= 0.f) t.predict_margin = d.predict_margin;
   if (t.predict_slack < 0) t.predict_slack = d.predict_slack;
   if (!(t.learned_load > 0.05f && t.learned_load < 0.95f)) t.learned_load = d.learned_load;
+  if (t.heavy_path != 0 && t.heavy_path != 1) return fail(ctx, SPG_ERR_INVALID_ARG, "heavy_path must be 0 or 1");
   ctx->tuning = t;
   return SPG_OK;
 }
@@ -149,7 +150,9 @@ spg_status spg_tune(spg_ctx* ctx, int32_t n, const spg_csr* A, const spg_csr* B,
   const spg_tuning saved = ctx->tuning;
   spg_tuning win = saved;
   double win_ms = 1e30;
-  const int tables[] = {1024, 2048, 4096};
+  // the batched path keeps every warp table size (see batched.cu), so only a
+  // single product searches the largest table
+  const std::vector<int> tables = n > 1 ? std::vector<int>{4096} : std::vector<int>{1024, 2048, 4096};
   const float loads[] = {0.35f, 0.5f, 0.65f};
   const int wpbs[] = {4, 8, 16};
   const int blocks[] = {8192, 16384};

@@ -388,6 +388,27 @@ def read_mtx(path: str) -> Csr:
     return Csr(int(s.rows), int(s.cols), rp, col, val)
 
 
+def transpose(m: Csr) -> Csr:
+    """Transpose of a host Csr with the library's host routine (no GPU needed)."""
+    L = _lib.load()
+    h = HostCsr(m)
+    src = h.struct()
+    t = _lib.SpgCsr()
+    st = L.spg_csr_transpose(ctypes.byref(src), ctypes.byref(t))
+    if st != _lib.SPG_OK:
+        raise SpgError(st, "spg_csr_transpose")
+    try:
+        rp = np.ctypeslib.as_array(ctypes.cast(t.row_ptr, ctypes.POINTER(ctypes.c_int64)), shape=(t.rows + 1,)).copy()
+        n = int(t.nnz)
+        col = np.ctypeslib.as_array(ctypes.cast(t.col_idx, ctypes.POINTER(ctypes.c_int32)), shape=(n,)).copy() \
+            if n else np.zeros(0, np.int32)
+        val = np.ctypeslib.as_array(ctypes.cast(t.val, ctypes.POINTER(ctypes.c_float)), shape=(n,)).copy() \
+            if n else np.zeros(0, np.float32)
+    finally:
+        L.spg_csr_free(None, ctypes.byref(t))
+    return Csr(int(t.rows), int(t.cols), rp, col, val)
+
+
 def write_mtx(path: str, m: Csr, drop_zeros: bool = False) -> None:
     """Writes a host Csr with the library's writer (no GPU needed)."""
     L = _lib.load()

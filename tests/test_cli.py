@@ -47,3 +47,22 @@ def test_cli_end_to_end(tmp_path, algo):
     np.testing.assert_array_equal(C.col_idx, R.col_idx)
     if algo != "cusparse":
         np.testing.assert_array_equal(C.val, R.val)  # shortest round-trip decimals
+
+
+@pytest.mark.gpu
+def test_cli_transpose_m2(tmp_path):
+    """C = A * A^T for a rectangular A read once (--transpose-m2)."""
+    from rtspmspm_b200 import transpose
+
+    A = gen.erdos_renyi(600, 900, 5.0, 12)
+    pa, pc, pl = (str(tmp_path / n) for n in ("a.mtx", "c.mtx", "log.txt"))
+    write_mtx(pa, A)
+    r = subprocess.run([CLI, "-m1", pa, "-m2", pa, "--transpose-m2", "-o", pc, "-l", pl, "--algo", "plain"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    C = read_mtx(pc)
+    R = oracle.spgemm(A, transpose(A))
+    assert (C.rows, C.cols) == (600, 600)
+    np.testing.assert_array_equal(C.row_ptr, R.row_ptr)
+    np.testing.assert_array_equal(C.col_idx, R.col_idx)
+    np.testing.assert_array_equal(C.val, R.val)

@@ -30,6 +30,8 @@ TUNINGS = {
     "default": {},
     "tiny_tables": {"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5},
     "mid_tables": {"warp_table_max": 256, "block_table_max": 2048, "max_load": 0.65, "warps_per_block": 4},
+    # heavy rows through the staged per-tile buckets instead of the rescanning tile kernel
+    "tiny_staged": {"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5, "heavy_path": 1},
 }
 
 
@@ -38,7 +40,7 @@ TUNINGS = {
 @pytest.mark.parametrize("name,A,B", PAIRS, ids=[p[0] for p in PAIRS])
 def test_parity(engine, name, A, B, algo, tuning):
     engine.set_tuning(**{**{"warp_table_max": 4096, "block_table_max": 16384, "max_load": 0.5,
-                            "warps_per_block": 8}, **TUNINGS[tuning]})
+                            "warps_per_block": 8, "heavy_path": 0}, **TUNINGS[tuning]})
     C, rep = engine.multiply(A, B, algo=algo, use_tuning=True, stage_timing=True)
     R = ref(name, A, B)
     assert_parity(C.to_host(), R)

@@ -196,3 +196,17 @@ def test_symmetric_file_in_slices_and_truncated_body(tmp_path):
     with pytest.raises(SpgError) as e:
         read_mtx(str(p))
     assert e.value.status == 5
+
+
+def test_transpose_matches_numpy():
+    from rtspmspm_b200 import transpose
+
+    for m in (gen.erdos_renyi(300, 170, 5.0, 3), gen.rmat(9, 8, seed=4), coo_to_csr(4, 6, [], [], [])):
+        t = transpose(m)
+        want = m.to_scipy().T.tocsr()
+        want.sort_indices()
+        assert (t.rows, t.cols, t.nnz) == (m.cols, m.rows, m.nnz)
+        np.testing.assert_array_equal(t.row_ptr, want.indptr)
+        np.testing.assert_array_equal(t.col_idx, want.indices)
+        np.testing.assert_array_equal(t.val, want.data.astype(np.float32))
+        assert t.to_scipy().T.toarray().tolist() == m.to_scipy().toarray().tolist()

@@ -174,12 +174,13 @@ spg_status spg_multiply_reuse(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, 
                               const spg_opts* opts, spg_report* report);
 
 /*
- * n independent products C[i] = A[i] * B[i] of uneven sizes in one
- * persistent launch per stage that drains a device queue of
- * (matrix, row-bin) tiles; with opts->use_graph the launch sequence is
- * captured once into a CUDA graph and replayed on later calls with the same
- * inputs.  Inputs must be on the device.  No reference counterpart (the
- * reference runs one product per process, scripts/AE_test.py:199-215).
+ * n independent products C[i] = A[i] * B[i] of uneven sizes: all rows of all
+ * products are binned together by table size and each stage runs one launch
+ * per table size over every product's rows of that bin (bin bounds read on
+ * the device); with opts->use_graph the launch sequence is captured once
+ * into a CUDA graph and replayed on later calls with the same inputs.
+ * Inputs must be on the device.  No reference counterpart (the reference
+ * runs one product per process, scripts/AE_test.py:199-215).
  */
 spg_status spg_multiply_batched(spg_ctx* ctx, int32_t n, const spg_csr* A, const spg_csr* B,
                                 spg_csr* C, const spg_opts* opts, spg_report* report);

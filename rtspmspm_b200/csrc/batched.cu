@@ -2,11 +2,12 @@
 //
 // No reference counterpart: the reference runs one product per process
 // (scripts/AE_test.py:199-215).  Here all rows of all products form one
-// global row space.  Each stage is ONE persistent launch whose CTAs drain a
-// device queue of (row-bin, row-range) tiles taken over every matrix at once
-// -- the widest tables first -- so small and large products share the GPU
-// without per-matrix launches.  The launch sequence is captured once into a
-// CUDA graph and replayed while the inputs stay the same.
+// global row space, binned by table size across every matrix at once; each
+// stage (symbolic, numeric) is one launch per warp-table size whose warps
+// stride over that bin's rows of all products, so small and large products
+// share the GPU without per-matrix launches.  Bin bounds are read on the
+// device, and the launch sequence is captured once into a CUDA graph and
+// replayed while the inputs stay the same.
 //
 // Plan (host, once per input set): matrix descriptors, global-row -> matrix
 // map, the nnz upper bound of every product (sum over rows of
@@ -36,11 +37,9 @@ struct BatchMat {
   int64_t rp_base;    // first entry of C_m's row pointers in the row-pointer slab
 };
 
+// Warps per CTA of the per-bin kernels; a CTA's tables stay within 96 KB.
 constexpr int kBatchWarps = 8;
-constexpr int kBatchArenaSmall = 64 * 1024;    // tables up to 2^kBatchSplitLog slots
-constexpr int kBatchArenaLarge = 192 * 1024;   // larger tables
-constexpr int kBatchSplitLog = 10;
-constexpr int kRowsPerWarpTile = 4;
+constexpr int kBatchCtaTableBytes = 96 * 1024;
 
 // Products per global row and the bound min(products, cols_m).
 __global__ void k_batch_products(const BatchMat* mats, const int32_t* row_mat, int64_t R, int64_t* prod,
@@ -78,95 +77,68 @@ __global__ void k_batch_bound_stats(const int32_t* row_mat, const int64_t* bound
   }
 }
 
-__device__ __forceinline__ int warps_usable(int logt, bool numeric, int arena_bytes) {
+// Warps per CTA for tables of 2^logt slots (keys only when symbolic; keys,
+// values and first-seen list when numeric).
+inline int batch_warps(int logt, bool numeric) {
   const int per_warp = (1 << logt) * (numeric ? 12 : 4);
-  int w = arena_bytes / per_warp;
-  return w < 1 ? 1 : (w > kBatchWarps ? kBatchWarps : w);
+  return std::max(1, std::min(kBatchWarps, kBatchCtaTableBytes / per_warp));
 }
 
-// Persistent symbolic (NUMERIC = false) or numeric (true) stage over the warp
-// bins [bin_lo, bin_hi].  Tile t maps to (bin, first row) with the
-// widest-table bins first.
-template <bool NUMERIC>
-__global__ void __launch_bounds__(kBatchWarps * 32, 2) k_batch_rows(const BatchMat* mats, const int32_t* row_mat,
-                                                                 const int32_t* lists, const int64_t* bin_off,
-                                                                 int bin_lo, int bin_hi, int arena_bytes,
-                                                                 int64_t* nnz, const int64_t* gscan, int32_t* c_col,
-                                                                 float* c_val, unsigned long long* ticket, int* flags) {
-  extern __shared__ int32_t arena[];
-  __shared__ int64_t sh_tiles[kNumWarpBins];
-  __shared__ unsigned long long sh_t;
-  const int lane = lane_id(), w = threadIdx.x >> 5;
-  if (threadIdx.x < kNumWarpBins) {
-    const int b = threadIdx.x;
-    const int64_t cnt = (b >= bin_lo && b <= bin_hi) ? bin_off[b + 1] - bin_off[b] : 0;
-    const int64_t per = (int64_t)warps_usable(kMinLogT + b, NUMERIC, arena_bytes) * kRowsPerWarpTile;
-    sh_tiles[b] = (cnt + per - 1) / per;
-  }
-  __syncthreads();
-  for (;;) {
-    if (threadIdx.x == 0) sh_t = atomicAdd(ticket, 1ull);
-    __syncthreads();
-    int64_t t = (int64_t)sh_t;
-    __syncthreads();
-    int bin = -1;
-    for (int b = kNumWarpBins - 1; b >= 0; --b) {
-      if (t < sh_tiles[b]) {
-        bin = b;
-        break;
-      }
-      t -= sh_tiles[b];
-    }
-    if (bin < 0) break;
-    const int logt = kMinLogT + bin;
-    const int usable = warps_usable(logt, NUMERIC, arena_bytes);
-    const int64_t per = (int64_t)usable * kRowsPerWarpTile;
-    const int64_t first = bin_off[bin] + t * per;
-    const int64_t last = min(first + per, bin_off[bin + 1]);
-    if (w < usable) {
-      const int T = 1 << logt;
-      int32_t* keys = arena + (size_t)w * T * (NUMERIC ? 3 : 1);
-      float* vals = reinterpret_cast<float*>(keys + T);
-      int32_t* list = keys + 2 * T;
-      for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
-      __syncwarp();
-      int epoch = 0;  // at most kRowsPerWarpTile rows per tile: no wrap
-      for (int64_t i = first + w; i < last; i += usable) {
-        const int64_t g = lists[i];
-        const BatchMat& M = mats[row_mat[g]];
-        const int32_t r = (int32_t)(g - M.row_start);
-        const int ep = M.B.cols < (1 << 24) ? epoch : kNoEpoch;
-        if (!NUMERIC) {
-          int cnt = 0;
-          switch (logt) {
-#define SPG_SYM(L)                                                                                    \
-  case L:                                                                                             \
-    cnt = symbolic_row<L, true>(M.A, M.B, r, keys, ep, flags);                                       \
-    break;
-            SPG_SYM(5) SPG_SYM(6) SPG_SYM(7) SPG_SYM(8) SPG_SYM(9) SPG_SYM(10) SPG_SYM(11) SPG_SYM(12)
-#undef SPG_SYM
-            default: break;
-          }
-          if (lane == 0) nnz[g] = cnt;
-        } else {
-          const int64_t base = gscan[M.row_start];
-          const int64_t off = M.c_base + (gscan[g] - base);
-          const int64_t want = gscan[g + 1] - gscan[g];
-          int e2 = ep;
-          switch (logt) {
-#define SPG_NUM(L)                                                                                      \
-  case L:                                                                                               \
-    numeric_row<L, true>(M.A, M.B, r, keys, vals, list, e2, c_col + off, c_val + off, want, flags);         \
-    break;
-            SPG_NUM(5) SPG_NUM(6) SPG_NUM(7) SPG_NUM(8) SPG_NUM(9) SPG_NUM(10) SPG_NUM(11) SPG_NUM(12)
-#undef SPG_NUM
-            default: break;
-          }
-        }
-        ++epoch;
+// Symbolic (NUMERIC = false) or numeric (true) pass over the rows of warp
+// bin LOGT of the global row space: warp per row, rows taken in stride from
+// the bin's list (its bounds read from bin_off on the device, so the launch
+// needs no host round trip and replays from a graph).  Each row looks up its
+// product's descriptor.  Tables are epoch-tagged while the product's B has
+// fewer than 2^24 columns; a row of a wider product clears the table first
+// if tagged keys may be left in it.
+template <int LOGT, bool NUMERIC>
+__global__ void __launch_bounds__(512, 2) k_batch_bin(const BatchMat* mats, const int32_t* row_mat,
+                                                      const int32_t* lists, const int64_t* bin_off, int64_t* nnz,
+                                                      const int64_t* gscan, int32_t* c_col, float* c_val,
+                                                      int* flags) {
+  constexpr int T = 1 << LOGT;
+  constexpr int kWords = NUMERIC ? numeric_words<LOGT>() : T;
+  extern __shared__ int32_t sm_tab[];
+  const int lane = lane_id();
+  int32_t* keys = sm_tab + (threadIdx.x >> 5) * kWords;
+  float* vals = reinterpret_cast<float*>(keys + T);
+  int32_t* list = keys + 2 * T;
+  for (int s2 = lane; s2 < T; s2 += 32) keys[s2] = kEmpty;
+  __syncwarp();
+  const int64_t first = bin_off[LOGT - kMinLogT], last = bin_off[LOGT - kMinLogT + 1];
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  int epoch = 0;
+  bool tagged = false;  // keys of an epoch may be in the table
+  for (int64_t i = first + gw; i < last; i += nw) {
+    const int64_t g = lists[i];
+    const BatchMat& M = mats[row_mat[g]];
+    const int32_t r = (int32_t)(g - M.row_start);
+    int ep = epoch;
+    if (M.B.cols >= (1 << 24)) {
+      ep = kNoEpoch;
+      if (tagged) {
+        for (int s2 = lane; s2 < T; s2 += 32) keys[s2] = kEmpty;
+        __syncwarp();
+        tagged = false;
+        epoch = 0;
       }
     }
-    __syncthreads();
+    if (!NUMERIC) {
+      const int cnt = symbolic_row<LOGT, true>(M.A, M.B, r, keys, ep, flags);
+      if (lane == 0) nnz[g] = cnt;
+    } else {
+      const int64_t base = gscan[M.row_start];
+      const int64_t off = M.c_base + (gscan[g] - base);
+      numeric_row<LOGT, true>(M.A, M.B, r, keys, vals, list, ep, c_col + off, c_val + off, gscan[g + 1] - gscan[g],
+                              flags);
+    }
+    if (ep >= 0) {
+      tagged = true;
+      if (!NUMERIC) next_row<LOGT>(keys, ep);
+      epoch = ep;
+      if (epoch == 0) tagged = false;  // wiped on wrap
+    }
   }
 }
 
@@ -217,6 +189,7 @@ struct BatchPlan {
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
   spg_tuning tune{};
+  int per_sm[2][kNumWarpBins] = {};  // CTAs per SM of the per-bin kernels (symbolic, numeric)
   int launches = 0;
 };
 
@@ -277,35 +250,36 @@ void enqueue(spg_ctx* ctx, BatchPlan* p) {
   int64_t* cursors = p->binmeta + 2 * kNumBins + 1;
   launch_binning(p->bound, R, INT64_MAX, kBinSymbolic, bp, p->bin_of_row, counts, offsets, cursors, p->lists, lc);
   launches += 3;
-  // each stage: one persistent launch for small tables, one for large ones
-  auto stage = [&](bool numeric, unsigned long long* ticket) {
-    for (int part = 0; part < 2; ++part) {
-      const int lo = part == 0 ? 0 : kBatchSplitLog - kMinLogT + 1;
-      const int hi = part == 0 ? kBatchSplitLog - kMinLogT : kNumWarpBins - 1;
-      const int arena = part == 0 ? kBatchArenaSmall : kBatchArenaLarge;
-      int per_sm = 0;
-      if (numeric)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_rows<true>, kBatchWarps * 32, arena);
-      else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_rows<false>, kBatchWarps * 32, arena);
-      const int grid = lc.sms * std::max(1, per_sm);
-      cudaMemsetAsync(ticket + part, 0, 8, lc.stream);
-      if (numeric)
-        k_batch_rows<true><<<grid, kBatchWarps * 32, arena, lc.stream>>>(
-            p->d_mats, p->row_mat, p->lists, offsets, lo, hi, arena, p->nnz, p->nnz, p->c_col, p->c_val,
-            ticket + part, ctx->d_flags);
-      else
-        k_batch_rows<false><<<grid, kBatchWarps * 32, arena, lc.stream>>>(
-            p->d_mats, p->row_mat, p->lists, offsets, lo, hi, arena, p->nnz, nullptr, nullptr, nullptr,
-            ticket + part, ctx->d_flags);
+  // each stage: one launch per warp-table size, each reading its bin's
+  // bounds on the device
+  auto stage = [&](bool numeric) {
+    for (int b = 0; b < kNumWarpBins; ++b) {
+      const int logt = kMinLogT + b;
+      const int w = batch_warps(logt, numeric);
+      const size_t smem = (size_t)w * (numeric ? 3 : 1) * ((size_t)1 << logt) * 4;
+      const int grid = lc.sms * p->per_sm[numeric ? 1 : 0][b];
+#define SPG_BB(L)                                                                                                 \
+  case L:                                                                                                         \
+    if (numeric)                                                                                                  \
+      k_batch_bin<L, true><<<grid, w * 32, smem, lc.stream>>>(p->d_mats, p->row_mat, p->lists, offsets, p->nnz,   \
+                                                              p->nnz, p->c_col, p->c_val, ctx->d_flags);          \
+    else                                                                                                          \
+      k_batch_bin<L, false><<<grid, w * 32, smem, lc.stream>>>(p->d_mats, p->row_mat, p->lists, offsets, p->nnz, \
+                                                               nullptr, nullptr, nullptr, ctx->d_flags);          \
+    break;
+      switch (logt) {
+        SPG_BB(5) SPG_BB(6) SPG_BB(7) SPG_BB(8) SPG_BB(9) SPG_BB(10) SPG_BB(11) SPG_BB(12)
+        default: break;
+      }
+#undef SPG_BB
       ++launches;
     }
   };
-  stage(false, ctx->d_counter + 4);
+  stage(false);
   launch_binning(p->nnz, R, INT64_MAX, kBinNumeric, bp, p->bin_of_row, counts, offsets, cursors, p->lists, lc);
   launch_excl_scan(p->nnz, R, p->nnz, p->scan_tmp, lc);
   launches += 7;
-  stage(true, ctx->d_counter + 6);
+  stage(true);
   k_batch_finalize<<<blocks_for(R + p->n, 256), 256, 0, lc.stream>>>(p->d_mats, p->n, p->row_mat, R, p->nnz,
                                                                      p->rp_out, p->nnz_m);
   ++launches;
@@ -320,8 +294,15 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
   std::unique_ptr<BatchPlan, void (*)(BatchPlan*)> guard(p, free_plan);
   p->n = n;
   p->key = plan_key(ctx, n, A, B, o);
-  p->tune = o.use_tuning ? ctx->tuning : default_tuning();
-  // every warp table size stays available on the persistent path: a smaller
+  if (o.use_tuning) {
+    p->tune = ctx->tuning;
+  } else {
+    // uneven products of short rows: fuller tables keep more warps per SM
+    // (load 0.65 measured best for the batch of 64 uneven products)
+    p->tune = default_tuning();
+    p->tune.max_load = 0.65f;
+  }
+  // every warp table size stays available on the batched path: a smaller
   // tuned maximum would send whole products to the one-by-one path
   p->tune.warp_table_max = default_tuning().warp_table_max;
   const BinParams bp = bin_params(p->tune);
@@ -439,10 +420,33 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
   SPG_CUDA(ctx, cudaMemcpyAsync(p->d_mats, p->mats.data(), (size_t)n * sizeof(BatchMat), cudaMemcpyHostToDevice,
                                 ctx->stream));
   SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     kBatchArenaLarge));
-  SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     kBatchArenaLarge));
+  // shared memory and CTAs per SM of every per-bin kernel (set before any capture)
+  for (int numeric = 0; numeric < 2; ++numeric) {
+    for (int b = 0; b < kNumWarpBins; ++b) {
+      const int logt = kMinLogT + b;
+      const int w = batch_warps(logt, numeric != 0);
+      const size_t smem = (size_t)w * (numeric ? 3 : 1) * ((size_t)1 << logt) * 4;
+      int per_sm = 0;
+#define SPG_BA(L)                                                                                             \
+  case L:                                                                                                     \
+    if (numeric) {                                                                                            \
+      SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_bin<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                         (int)smem));                                                         \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_bin<L, true>, w * 32, smem);             \
+    } else {                                                                                                  \
+      SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_bin<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                         (int)smem));                                                         \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_bin<L, false>, w * 32, smem);            \
+    }                                                                                                         \
+    break;
+      switch (logt) {
+        SPG_BA(5) SPG_BA(6) SPG_BA(7) SPG_BA(8) SPG_BA(9) SPG_BA(10) SPG_BA(11) SPG_BA(12)
+        default: break;
+      }
+#undef SPG_BA
+      p->per_sm[numeric][b] = std::max(1, per_sm);
+    }
+  }
   SPG_TRY(dmalloc(ctx, p, &p->nnz, (size_t)R + 1));
   SPG_TRY(dmalloc(ctx, p, &p->bin_of_row, (size_t)std::max<int64_t>(R, 1)));
   SPG_TRY(dmalloc(ctx, p, &p->binmeta, (size_t)(3 * kNumBins + 1)));

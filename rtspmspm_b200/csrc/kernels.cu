@@ -664,6 +664,20 @@ template <typename Off>
 __device__ __forceinline__ void tile_segment(const DCsr& B, Off bs, int len, float a, int32_t c0, float* acc,
                                              uint32_t* bits, int* flags) {
   const int lane = lane_id();
+  if (len <= 32) {
+    // one round: a single load per lane
+    if (lane < len) {
+      const int32_t off = B.col[bs + lane] - c0;
+      const float pr = prod_rn(a, B.val[bs + lane]);
+      if ((uint32_t)off < (uint32_t)kTileCols) {
+        acc[off] = add_rn(acc[off], pr);
+        atomicOr(&bits[off >> 5], 1u << (off & 31));
+      } else {
+        raise_flag(flags, kFlagBadIndex);
+      }
+    }
+    return;
+  }
   for (int q0 = 0; q0 < len; q0 += 4 * 32) {
     int32_t off[4];
     float pr[4];
@@ -824,6 +838,8 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
         len = (int)(re - rs);
       }
       const int n = (int)min((int64_t)32, e - base);
+      // none of these B rows reaches into the tile: next chunk
+      if (!__any_sync(kFull, len > 0)) continue;
       const unsigned long_mask = __ballot_sync(kFull, len >= kTileLongSeg);
       int idx = 0;
       while (idx < n) {

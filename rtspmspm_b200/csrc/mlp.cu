@@ -315,12 +315,14 @@ __device__ __forceinline__ void capacity_of(int64_t p, int64_t cols, float o0, f
 
 // Learned plan: per 16-row tile, the warp computes each row's features and
 // products, runs the MLP on the tile with tensor cores, and writes the
-// products, capacity and exact-path mark of every row.
+// products, capacity and exact-path mark of every row; n_exact counts the
+// rows marked for the exact path.
 template <bool R32>
 __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B, const __nv_bfloat16* w,
                                                                   float margin, int slack, int64_t warp_cap,
                                                                   int force_overflow, int64_t* prod, int64_t* cap,
-                                                                  uint8_t* need_exact) {
+                                                                  uint8_t* need_exact,
+                                                                  unsigned long long* n_exact) {
   __shared__ MlpSmem sm;
   __shared__ float tile[kPlanWarps][16 * kMlpIn];
   __shared__ int64_t tprod[kPlanWarps][16];
@@ -354,6 +356,7 @@ __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B
         prod[ra] = tprod[wib][ia];
         cap[ra] = c;
         need_exact[ra] = ex;
+        if (ex) atomicAdd(n_exact, 1ull);
       }
       if (rb < rows) {
         int64_t c;
@@ -362,6 +365,7 @@ __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B
         prod[rb] = tprod[wib][ib];
         cap[rb] = c;
         need_exact[rb] = ex;
+        if (ex) atomicAdd(n_exact, 1ull);
       }
     }
     __syncwarp();
@@ -563,16 +567,19 @@ void launch_mlp_predict(const void* w16, const float* feats, int64_t rows, float
 }
 
 void launch_learned_plan(const DCsr& A, const DCsr& B, const void* w16, float margin, int slack, int64_t warp_cap,
-                         int force_overflow, int64_t* prod, int64_t* cap, uint8_t* need_exact, const LaunchCtx& lc) {
+                         int force_overflow, int64_t* prod, int64_t* cap, uint8_t* need_exact,
+                         unsigned long long* n_exact, const LaunchCtx& lc) {
   if (A.rows == 0) return;
   const int64_t tiles = (A.rows + 15) / 16;
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((tiles + kPlanWarps - 1) / kPlanWarps, lc.sms * 8));
   if (B.rp32)
     k_learned_plan<true><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(A, B, (const __nv_bfloat16*)w16, margin, slack,
-                                                                    warp_cap, force_overflow, prod, cap, need_exact);
+                                                                    warp_cap, force_overflow, prod, cap, need_exact,
+                                                                    n_exact);
   else
     k_learned_plan<false><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(A, B, (const __nv_bfloat16*)w16, margin, slack,
-                                                                     warp_cap, force_overflow, prod, cap, need_exact);
+                                                                     warp_cap, force_overflow, prod, cap, need_exact,
+                                                                     n_exact);
 }
 
 void launch_mlp_fwd_bwd(const void* w16, const float* feats, const float* targets, int64_t n, float* work,

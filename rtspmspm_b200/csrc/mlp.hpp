@@ -17,7 +17,8 @@ void launch_features(const DCsr& A, const DCsr& B, float* feats, int64_t* prod, 
 void launch_mlp_predict(const void* w16, const float* feats, int64_t rows, float* out, const LaunchCtx& lc);
 // Fused learned plan: per row products, MLP capacity and exact-path mark.
 void launch_learned_plan(const DCsr& A, const DCsr& B, const void* w16, float margin, int slack, int64_t warp_cap,
-                         int force_overflow, int64_t* prod, int64_t* cap, uint8_t* need_exact, const LaunchCtx& lc);
+                         int force_overflow, int64_t* prod, int64_t* cap, uint8_t* need_exact,
+                         unsigned long long* n_exact, const LaunchCtx& lc);
 // Forward + backward over n rows; `work` holds mlp_work_floats(n) floats;
 // grad gets the full gradient (overwritten); loss (device) the mean loss.
 void launch_mlp_fwd_bwd(const void* w16, const float* feats, const float* targets, int64_t n, float* work,

@@ -156,6 +156,22 @@ spg_status spg_multiply(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_cs
                         const spg_opts* opts, spg_report* report);
 
 /*
+ * C = A * B delivered into caller-owned host buffers, with the device-to-host
+ * copy of C overlapped with the product: A's rows are taken in `blocks`
+ * row blocks, and each block's part of C is copied on a second stream while
+ * the next block is computed.  C->row_ptr (rows+1 entries of C->index_bits
+ * width), C->col_idx and C->val (C->capacity entries) are host memory
+ * (pinned memory gives the full host-link bandwidth); on success C->rows,
+ * C->cols and C->nnz are set.  With too small a capacity the call fails
+ * with SPG_ERR_INVALID_ARG and C->nnz holds the size needed.  A and B given
+ * by the same descriptor are uploaded once.  Plain or learned method.
+ * Replaces the reference's compute-then-copy sequence (optixSpMSpM.cpp:
+ * 585-611 then printResult's device-to-host copy :462-463).
+ */
+spg_status spg_multiply_into_host(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_csr* C,
+                                  int32_t blocks, const spg_opts* opts, spg_report* report);
+
+/*
  * Value-only recompute: C already holds the structure of A * B (the result
  * of an earlier spg_multiply on matrices with the same structure as A and
  * B, on the device, either index width).  Recomputes C->val in place from

@@ -105,6 +105,8 @@ SIGNATURES = [
     ("spg_get_stream", _vp, [_vp]),
     ("spg_multiply", ctypes.c_int32, [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
     ("spg_csr_transpose", ctypes.c_int32, [_P(SpgCsr), _P(SpgCsr)]),
+    ("spg_multiply_into_host", ctypes.c_int32,
+     [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), ctypes.c_int32, _P(SpgOpts), _P(SpgReport)]),
     ("spg_multiply_reuse", ctypes.c_int32, [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
     ("spg_multiply_batched", ctypes.c_int32,
      [_vp, ctypes.c_int32, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),

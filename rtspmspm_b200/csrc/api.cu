@@ -105,6 +105,13 @@ spg_status read_flags(spg_ctx* ctx, int* flags) {
   return SPG_OK;
 }
 
+// A and B describe the same matrix (same storage): prepare it once.
+bool same_matrix(const spg_csr* a, const spg_csr* b) {
+  return a == b || (a->rows == b->rows && a->cols == b->cols && a->nnz == b->nnz && a->index_bits == b->index_bits &&
+                    a->location == b->location && a->row_ptr == b->row_ptr && a->col_idx == b->col_idx &&
+                    a->val == b->val);
+}
+
 spg_status prepare_matrix(spg_ctx* ctx, const spg_csr* m, DevMat& out, bool validate) {
   if (!m) return fail(ctx, SPG_ERR_INVALID_ARG, "null matrix");
   if (m->rows < 0 || m->cols < 0 || m->nnz < 0) return fail(ctx, SPG_ERR_INVALID_ARG, "negative dimension");
@@ -689,6 +696,10 @@ spg_status spg_destroy(spg_ctx* ctx) {
   cudaFree(ctx->d_flags);
   cudaFree(ctx->d_counter);
   cudaFreeHost(ctx->h_stage);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return SPG_OK;
@@ -724,12 +735,15 @@ spg_status spg_multiply(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_cs
   StageTimer outer(ctx, false);
   DevMat dA, dB;
   SPG_TRY(prepare_matrix(ctx, A, dA, !o.skip_validation));
-  SPG_TRY(prepare_matrix(ctx, B, dB, !o.skip_validation));
+  // C = A*A through one descriptor: prepared (uploaded) once
+  const bool same = same_matrix(A, B);
+  if (!same) SPG_TRY(prepare_matrix(ctx, B, dB, !o.skip_validation));
+  const DevMat& rB = same ? dA : dB;
   if (!o.skip_validation) SPG_TRY(check_flags(ctx, report));
   spg_csr dev_c{};
   spg_status st;
-  if (o.algo == SPG_ALGO_CUSPARSE) st = multiply_cusparse(ctx, dA, dB, &dev_c, o, report);
-  else if (o.algo == SPG_ALGO_PLAIN || o.algo == SPG_ALGO_LEARNED) st = multiply_device(ctx, dA, dB, &dev_c, o, report);
+  if (o.algo == SPG_ALGO_CUSPARSE) st = multiply_cusparse(ctx, dA, rB, &dev_c, o, report);
+  else if (o.algo == SPG_ALGO_PLAIN || o.algo == SPG_ALGO_LEARNED) st = multiply_device(ctx, dA, rB, &dev_c, o, report);
   else return fail(ctx, SPG_ERR_INVALID_ARG, "unknown algo %d", o.algo);
   if (st != SPG_OK) {
     spg_csr_free(ctx, &dev_c);
@@ -751,6 +765,139 @@ spg_status spg_multiply(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_cs
     float ms = 0.f;
     (void)ms;
   }
+  return SPG_OK;
+}
+
+spg_status spg_multiply_into_host(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, spg_csr* C, int32_t blocks,
+                                  const spg_opts* opts, spg_report* report) {
+  if (!ctx) return SPG_ERR_INVALID_ARG;
+  if (!A || !B || !C) return fail(ctx, SPG_ERR_INVALID_ARG, "null argument");
+  if (A->cols != B->rows)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "inner dimensions differ (%lld vs %lld)", (long long)A->cols,
+                (long long)B->rows);
+  if (C->location != SPG_HOST) return fail(ctx, SPG_ERR_INVALID_ARG, "C must describe host buffers");
+  if (C->index_bits != 32 && C->index_bits != 64) return fail(ctx, SPG_ERR_INVALID_ARG, "bad C index_bits");
+  if (!C->row_ptr || C->capacity < 0 || (C->capacity > 0 && (!C->col_idx || !C->val)))
+    return fail(ctx, SPG_ERR_INVALID_ARG, "C needs row_ptr and, with a capacity, col_idx/val buffers");
+  if (blocks < 1) return fail(ctx, SPG_ERR_INVALID_ARG, "blocks must be >= 1");
+  if (A->rows > INT32_MAX) return fail(ctx, SPG_ERR_UNSUPPORTED, "more than 2^31-1 rows");
+  spg_opts o{};
+  if (opts) o = *opts;
+  if (o.algo != SPG_ALGO_PLAIN && o.algo != SPG_ALGO_LEARNED)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "spg_multiply_into_host runs the plain or learned method");
+  o.out_location = SPG_DEVICE;
+  o.out_index_bits = 64;
+  SPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (report) {
+    std::memset(report, 0, sizeof *report);
+    report->algo = o.algo;
+    report->rows = A->rows;
+  }
+  const int launches0 = ctx->launches;
+  DevMat dA, dB;
+  SPG_TRY(prepare_matrix(ctx, A, dA, !o.skip_validation));
+  const bool same = same_matrix(A, B);
+  if (!same) SPG_TRY(prepare_matrix(ctx, B, dB, !o.skip_validation));
+  const DevMat& rB = same ? dA : dB;
+  if (!o.skip_validation) SPG_TRY(check_flags(ctx, report));
+  if (!ctx->copy_stream) SPG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  const LaunchCtx lc = launch_ctx(ctx);
+  const int64_t rows = A->rows;
+  const int w = C->index_bits / 8;
+  char* host_rp = static_cast<char*>(C->row_ptr);
+  C->rows = rows;
+  C->cols = B->cols;
+  if (rows == 0) {
+    if (w == 8) *static_cast<int64_t*>(C->row_ptr) = 0;
+    else *static_cast<int32_t*>(C->row_ptr) = 0;
+    C->nnz = 0;
+    return SPG_OK;
+  }
+  const int64_t nb = std::min<int64_t>(blocks, rows);
+  DevBuf rp_dev;  // C's row pointers in C's width, staged for the copies
+  SPG_TRY(rp_dev.alloc(ctx, (size_t)(rows + 1) * w));
+  std::vector<cudaEvent_t> evs;
+  std::vector<spg_csr> parts;  // device parts of C whose copies are in flight
+  auto drain = [&]() {
+    cudaStreamSynchronize(ctx->copy_stream);
+    for (cudaEvent_t e : evs) cudaEventDestroy(e);
+    evs.clear();
+    for (spg_csr& c : parts) spg_csr_free(ctx, &c);
+    parts.clear();
+  };
+  int64_t offset = 0;
+  bool overflow = false;
+  spg_status st = SPG_OK;
+  for (int64_t b = 0; b < nb && st == SPG_OK; ++b) {
+    const int64_t r0 = rows * b / nb, r1 = rows * (b + 1) / nb;
+    DevMat Ab;  // view of A's rows [r0, r1): row pointers index the full column/value arrays
+    Ab.view = dA.view;
+    Ab.view.rows = r1 - r0;
+    Ab.view.rp = dA.view.rp + r0;
+    Ab.view.rp32 = dA.view.rp32 ? dA.view.rp32 + r0 : nullptr;
+    Ab.nnz = dA.nnz;
+    spg_csr cb{};
+    spg_report rb{};
+    st = multiply_device(ctx, Ab, rB, &cb, o, report ? &rb : nullptr);
+    if (st != SPG_OK) {
+      spg_csr_free(ctx, &cb);
+      break;
+    }
+    if (report) {
+      report->products += rb.products;
+      report->ms_total += rb.ms_total;
+      report->rows_predicted += rb.rows_predicted;
+      report->rows_overflow += rb.rows_overflow;
+      report->rows_heavy += rb.rows_heavy;
+      report->device_flags |= rb.device_flags;
+      for (int s = 0; s < SPG_STAGE_COUNT; ++s) report->ms_stage[s] += rb.ms_stage[s];
+      for (int s = 0; s < SPG_NUM_BINS; ++s) report->bin_rows[s] += rb.bin_rows[s];
+    }
+    if (!overflow && offset + cb.nnz <= C->capacity) {
+      // this block's rows of C (its last row pointer too for the final block)
+      const int64_t n_rp = (r1 == rows) ? (r1 - r0 + 1) : (r1 - r0);
+      launch_shift_rp(static_cast<const int64_t*>(cb.row_ptr), n_rp, offset, rp_dev.as<char>() + (size_t)r0 * w,
+                      C->index_bits, lc);
+      ++ctx->launches;
+      cudaEvent_t ev = nullptr;
+      st = cuda_status(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+      if (st != SPG_OK) {
+        spg_csr_free(ctx, &cb);
+        break;
+      }
+      evs.push_back(ev);
+      cudaEventRecord(ev, ctx->stream);
+      cudaStreamWaitEvent(ctx->copy_stream, ev, 0);
+      cudaMemcpyAsync(host_rp + (size_t)r0 * w, rp_dev.as<char>() + (size_t)r0 * w, (size_t)n_rp * w,
+                      cudaMemcpyDeviceToHost, ctx->copy_stream);
+      if (cb.nnz) {
+        cudaMemcpyAsync(C->col_idx + offset, cb.col_idx, (size_t)cb.nnz * 4, cudaMemcpyDeviceToHost,
+                        ctx->copy_stream);
+        cudaMemcpyAsync(C->val + offset, cb.val, (size_t)cb.nnz * 4, cudaMemcpyDeviceToHost, ctx->copy_stream);
+      }
+      // kept until every copy is done: freeing it on the copy stream would let
+      // the pool hand its memory to the next block's compute with a wait on
+      // this copy, serializing the two
+      parts.push_back(cb);
+    } else {
+      overflow = true;
+      spg_csr_free(ctx, &cb);
+    }
+    offset += cb.nnz;
+  }
+  // the staged row pointers are freed on ctx->stream: order it after the copies
+  drain();
+  if (st != SPG_OK) return st;
+  SPG_CUDA(ctx, cudaGetLastError());
+  C->nnz = offset;
+  if (report) {
+    report->nnz_c = offset;
+    report->kernel_launches = ctx->launches - launches0;
+  }
+  if (overflow)
+    return fail(ctx, SPG_ERR_INVALID_ARG,
+                "C needs room for %lld entries but its capacity is %lld (C->nnz holds the size needed)",
+                (long long)offset, (long long)C->capacity);
   return SPG_OK;
 }
 
@@ -780,9 +927,10 @@ spg_status spg_multiply_reuse(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, 
   const int launches0 = ctx->launches;
   DevMat dA, dB;
   SPG_TRY(prepare_matrix(ctx, A, dA, !o.skip_validation));
-  SPG_TRY(prepare_matrix(ctx, B, dB, !o.skip_validation));
+  const bool same = same_matrix(A, B);
+  if (!same) SPG_TRY(prepare_matrix(ctx, B, dB, !o.skip_validation));
   if (!o.skip_validation) SPG_TRY(check_flags(ctx, report));
-  SPG_TRY(spg::multiply_reuse_device(ctx, dA, dB, C, o, report));
+  SPG_TRY(spg::multiply_reuse_device(ctx, dA, same ? dA : dB, C, o, report));
   if (report) report->kernel_launches = ctx->launches - launches0;
   return SPG_OK;
 }

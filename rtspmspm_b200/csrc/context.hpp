@@ -19,6 +19,7 @@ struct spg_ctx {
   int sms = 148;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // device-to-host copies overlapped with compute (created on first use)
   cudaMemPool_t pool = nullptr;
   std::string last_error;
   std::string gpu_name;
@@ -98,6 +99,9 @@ struct DevMat {
 // pointers.  `validate` runs the structure check kernel (flags raised on the
 // context's device flag word).
 spg_status prepare_matrix(spg_ctx* ctx, const spg_csr* m, DevMat& out, bool validate);
+
+// A and B describe the same matrix (same storage): prepare it once.
+bool same_matrix(const spg_csr* a, const spg_csr* b);
 
 // Reads and clears the device flag word.
 spg_status read_flags(spg_ctx* ctx, int* flags);

@@ -329,6 +329,13 @@ __device__ __forceinline__ void cta_for_each_product(const DCsr& A, const DCsr& 
         // starts of the segments after kc, kc + 1, ..., kc + 31
         const int wi = kc + 1 + lane;
         const Off nxt = wi <= cnt ? sh_excl[wi] : (Off)(R32 ? 0x7fffffff : INT64_MAX);
+        // the next 32 products all inside segment kc (long rows of B): no search
+        const Off seg_end = __shfl_sync(kFull, nxt, 0);
+        if (pos >= sh_excl[kc] && pos + 32 <= seg_end && pos + 32 <= hi) {
+          f(B.col[sh_bs[kc] + (pos - sh_excl[kc]) + (Off)lane]);
+          pos += 32;
+          continue;
+        }
         const Off wend = __shfl_sync(kFull, nxt, 31);
         if (wend <= pos) {
           // more than 31 empty segments in a row: slide the window on
@@ -1136,6 +1143,20 @@ void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int3
     default: break;
   }
 #undef SPG_NWL
+}
+
+// out[i] = in[i] + off as int32 (out_bits 32) or int64.
+__global__ void k_shift_rp(const int64_t* in, int64_t n, int64_t off, void* out, int out_bits) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = in[i] + off;
+    if (out_bits == 32) static_cast<int32_t*>(out)[i] = (int32_t)v;
+    else static_cast<int64_t*>(out)[i] = v;
+  }
+}
+
+void launch_shift_rp(const int64_t* in, int64_t n, int64_t off, void* out, int out_bits, const LaunchCtx& lc) {
+  if (n == 0) return;
+  k_shift_rp<<<grid_for(n, 256, 1, lc.sms * 8), 256, 0, lc.stream>>>(in, n, off, out, out_bits);
 }
 
 void launch_row_lengths(const int64_t* rp, int64_t rows, int64_t* len, const LaunchCtx& lc) {

@@ -237,6 +237,39 @@ class Engine:
                                         ctypes.byref(o), ctypes.byref(rep)))
         return Result(self, c), rep.as_dict()
 
+    def multiply_into_host(self, A, B, row_ptr, col_idx, val, blocks: int = 8, index_bits: int = 64, **kw):
+        """C = A*B written into caller host arrays (numpy or pinned torch tensors,
+        len(col_idx) = capacity), the download overlapped with the product in
+        `blocks` row blocks. Returns (nnz, report dict)."""
+        sa, ka = self._as_struct(A, self.device)
+        sb, kb = self._as_struct(B, self.device) if B is not A else (sa, ka)
+        c = self._host_out(row_ptr, col_idx, val, index_bits)
+        o = self.opts(**kw)
+        rep = _lib.SpgReport()
+        self._check(self.L.spg_multiply_into_host(self.ctx, ctypes.byref(sa), ctypes.byref(sb), ctypes.byref(c),
+                                                  int(blocks), ctypes.byref(o), ctypes.byref(rep)))
+        return int(c.nnz), rep.as_dict()
+
+    def multiply_into_host_raw(self, sa: _lib.SpgCsr, sb: _lib.SpgCsr, c: _lib.SpgCsr, blocks: int,
+                               o: _lib.SpgOpts, rep: _lib.SpgReport) -> None:
+        """Low-overhead call on prepared structs (benchmark loops)."""
+        self._check(self.L.spg_multiply_into_host(self.ctx, ctypes.byref(sa), ctypes.byref(sb), ctypes.byref(c),
+                                                  int(blocks), ctypes.byref(o), ctypes.byref(rep)))
+
+    @staticmethod
+    def _host_out(row_ptr, col_idx, val, index_bits: int) -> _lib.SpgCsr:
+        def ptr(x):
+            return x.data_ptr() if hasattr(x, "data_ptr") else x.ctypes.data
+
+        c = _lib.SpgCsr()
+        c.index_bits = index_bits
+        c.location = _lib.SPG_HOST
+        c.row_ptr = ptr(row_ptr)
+        c.col_idx = ptr(col_idx) if len(col_idx) else 0
+        c.val = ptr(val) if len(val) else 0
+        c.capacity = len(col_idx)
+        return c
+
     def multiply_reuse(self, A, B, C: "Result", **kw):
         """Recomputes the values of C = A*B in place; C (a device Result of an
         earlier multiply) holds the structure of A*B. Returns the report dict."""

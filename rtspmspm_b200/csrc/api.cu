@@ -95,8 +95,19 @@ static int block_table_log(const spg_tuning& t) {
   return ilog2_floor(std::max(1024, std::min(32768, t.block_table_max)));
 }
 
+// Small device-to-host reads (bin offsets, totals, flags) are written into
+// the pinned staging words by a one-block kernel through the mapped host
+// address, not by a copy engine: a large device-to-host copy in flight on
+// another stream (spg_multiply_into_host) would otherwise delay them.
+spg_status stage_read(spg_ctx* ctx, void* host_dst, const void* dev_src, size_t bytes) {
+  const size_t at = (size_t)(static_cast<char*>(host_dst) - reinterpret_cast<char*>(ctx->h_stage));
+  if (at + bytes > 64 * sizeof(int64_t) || (bytes & 3)) return fail(ctx, SPG_ERR_INTERNAL, "bad staging read");
+  launch_copy_words(dev_src, reinterpret_cast<char*>(ctx->h_stage_dev) + at, (int64_t)(bytes / 4), launch_ctx(ctx));
+  return cuda_status(ctx, cudaGetLastError(), "stage_read");
+}
+
 spg_status read_flags(spg_ctx* ctx, int* flags) {
-  SPG_CUDA(ctx, cudaMemcpyAsync(&ctx->h_stage[15], ctx->d_flags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  SPG_TRY(stage_read(ctx, &ctx->h_stage[15], ctx->d_flags, sizeof(int)));
   SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   int f = 0;
   std::memcpy(&f, &ctx->h_stage[15], sizeof(int));
@@ -270,11 +281,9 @@ struct Pipeline {
 
   // Offsets of the last binning (and optional extra int64 words) to host.
   spg_status fetch_offsets(const int64_t* extra = nullptr, int64_t* extra_host = nullptr, int n_extra = 0) {
-    SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage, offsets(), sizeof(int64_t) * (kNumBins + 1), cudaMemcpyDeviceToHost,
-                                  ctx->stream));
+    SPG_TRY(stage_read(ctx, ctx->h_stage, offsets(), sizeof(int64_t) * (kNumBins + 1)));
     for (int i = 0; i < n_extra; ++i)
-      SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kNumBins + 1 + i, extra + i, sizeof(int64_t),
-                                    cudaMemcpyDeviceToHost, ctx->stream));
+      SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 1 + i, extra + i, sizeof(int64_t)));
     SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     std::memcpy(h_off, ctx->h_stage, sizeof(int64_t) * (kNumBins + 1));
     for (int i = 0; i < n_extra; ++i) extra_host[i] = ctx->h_stage[kNumBins + 1 + i];
@@ -425,10 +434,9 @@ spg_status multiply_plain(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opts&
   int64_t extra[2];
   const int64_t* src[2] = {P.nnz.as<int64_t>() + P.rows, reinterpret_cast<const int64_t*>(ctx->d_counter + 1)};
   // fetch offsets + total nnz + products
-  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage, P.offsets(), sizeof(int64_t) * (kNumBins + 1), cudaMemcpyDeviceToHost,
-                                ctx->stream));
-  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kNumBins + 1, src[0], 8, cudaMemcpyDeviceToHost, ctx->stream));
-  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kNumBins + 2, src[1], 8, cudaMemcpyDeviceToHost, ctx->stream));
+  SPG_TRY(stage_read(ctx, ctx->h_stage, P.offsets(), sizeof(int64_t) * (kNumBins + 1)));
+  SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 1, src[0], 8));
+  SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 2, src[1], 8));
   SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   std::memcpy(P.h_off, ctx->h_stage, sizeof(int64_t) * (kNumBins + 1));
   extra[0] = ctx->h_stage[kNumBins + 1];
@@ -476,8 +484,7 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
   ctx->launches += 4;
   int64_t slab_total = 0;
   constexpr int kExactSlot = 40, kRetrySlot = 41;  // h_stage words (64 in all)
-  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kExactSlot, ctx->d_counter + 3, 8, cudaMemcpyDeviceToHost,
-                                ctx->stream));
+  SPG_TRY(stage_read(ctx, ctx->h_stage + kExactSlot, ctx->d_counter + 3, 8));
   SPG_TRY(P.fetch_offsets(slab_off.as<int64_t>() + rows, &slab_total, 1));
   const int64_t n_exact = ctx->h_stage[kExactSlot];
   int64_t light = 0;
@@ -501,8 +508,7 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
   tm.mark(SPG_STAGE_FIXUP);
   bool exact_needed = n_exact > 0;
   if (!exact_needed) {
-    SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kRetrySlot, ctx->d_counter + 2, 8, cudaMemcpyDeviceToHost,
-                                  ctx->stream));
+    SPG_TRY(stage_read(ctx, ctx->h_stage + kRetrySlot, ctx->d_counter + 2, 8));
     SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     exact_needed = ctx->h_stage[kRetrySlot] > 0;
   }
@@ -527,12 +533,9 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
   tm.mark(SPG_STAGE_SCAN);
   launch_excl_scan(P.nnz.as<int64_t>(), rows, P.nnz.as<int64_t>(), P.scan_tmp.as<int64_t>(), lc);
   ctx->launches += 4;
-  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage, P.offsets(), sizeof(int64_t) * (kNumBins + 1), cudaMemcpyDeviceToHost,
-                                ctx->stream));
-  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kNumBins + 1, P.nnz.as<int64_t>() + rows, 8, cudaMemcpyDeviceToHost,
-                                ctx->stream));
-  SPG_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage + kNumBins + 2, ctx->d_counter + 1, 16, cudaMemcpyDeviceToHost,
-                                ctx->stream));
+  SPG_TRY(stage_read(ctx, ctx->h_stage, P.offsets(), sizeof(int64_t) * (kNumBins + 1)));
+  SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 1, P.nnz.as<int64_t>() + rows, 8));
+  SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 2, ctx->d_counter + 1, 16));
   SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (exact_needed) std::memcpy(P.h_off, ctx->h_stage, sizeof(int64_t) * (kNumBins + 1));
   const int64_t total = ctx->h_stage[kNumBins + 1];
@@ -680,7 +683,9 @@ spg_status spg_create(spg_ctx** out, int32_t device) {
   SPG_CUDA(ctx.get(), cudaMemset(ctx->d_flags, 0, 64));
   SPG_CUDA(ctx.get(), cudaMalloc(&ctx->d_counter, 8 * sizeof(unsigned long long)));
   SPG_CUDA(ctx.get(), cudaMemset(ctx->d_counter, 0, 8 * sizeof(unsigned long long)));
-  SPG_CUDA(ctx.get(), cudaMallocHost(&ctx->h_stage, 64 * sizeof(int64_t)));
+  // mapped, so small read-backs can be written by a kernel (stage_read)
+  SPG_CUDA(ctx.get(), cudaHostAlloc((void**)&ctx->h_stage, 64 * sizeof(int64_t), cudaHostAllocMapped));
+  SPG_CUDA(ctx.get(), cudaHostGetDevicePointer((void**)&ctx->h_stage_dev, ctx->h_stage, 0));
   ctx->tuning = default_tuning();
   *out = ctx.release();
   return SPG_OK;

@@ -32,7 +32,8 @@ struct spg_ctx {
   int* d_flags = nullptr;
   unsigned long long* d_counter = nullptr;  // tile queue / retry counters (4 entries)
   // pinned host staging for small device->host reads
-  int64_t* h_stage = nullptr;
+  int64_t* h_stage = nullptr;      // 64 words, mapped
+  int64_t* h_stage_dev = nullptr;  // the same words seen from the device
   int launches = 0;
   // batched-launch graph cache
   void* batch_cache = nullptr;

@@ -1145,6 +1145,17 @@ void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int3
 #undef SPG_NWL
 }
 
+// dst[i] = src[i] for n 32-bit words; dst may be mapped pinned host memory.
+__global__ void k_copy_words(const uint32_t* src, uint32_t* dst, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+void launch_copy_words(const void* src, void* dst, int64_t n, const LaunchCtx& lc) {
+  if (n == 0) return;
+  k_copy_words<<<1, 128, 0, lc.stream>>>(static_cast<const uint32_t*>(src), static_cast<uint32_t*>(dst), n);
+}
+
 // out[i] = in[i] + off as int32 (out_bits 32) or int64.
 __global__ void k_shift_rp(const int64_t* in, int64_t n, int64_t off, void* out, int out_bits) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {

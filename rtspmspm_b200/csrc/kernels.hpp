@@ -71,6 +71,9 @@ void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int3
                              const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
                              int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
                              const LaunchCtx& lc, int wpb);
+// Copies n 32-bit words with one small kernel (dst may be mapped pinned host
+// memory: the read-back then needs no copy engine).
+void launch_copy_words(const void* src, void* dst, int64_t n, const LaunchCtx& lc);
 // Row pointers shifted by `off` into an int32 (out_bits 32) or int64 array.
 void launch_shift_rp(const int64_t* in, int64_t n, int64_t off, void* out, int out_bits, const LaunchCtx& lc);
 // Value-only recompute: row lengths of C, and heavy-row slots and per-tile

@@ -66,3 +66,31 @@ def test_cli_transpose_m2(tmp_path):
     np.testing.assert_array_equal(C.row_ptr, R.row_ptr)
     np.testing.assert_array_equal(C.col_idx, R.col_idx)
     np.testing.assert_array_equal(C.val, R.val)
+
+
+@pytest.mark.gpu
+def test_ae_harness_with_the_cli(tmp_path):
+    """The AE_test-compatible harness driving the real CLI (cuSPARSE vs the
+    learned method): CSV files written, square and rectangular datasets."""
+    import csv
+
+    from rtspmspm_b200 import ae_harness
+
+    d = tmp_path / "data"
+    (d / "sq").mkdir(parents=True)
+    write_mtx(str(d / "sq" / "sq.mtx"), gen.erdos_renyi(1200, 1200, 5.0, 3))
+    write_mtx(str(d / "rect.mtx"), gen.erdos_renyi(1500, 900, 4.0, 4))
+    out = tmp_path / "result"
+    used, failed = ae_harness.profile(str(d), str(out), ae_harness.default_programs(), runs=2, log=lambda *a: None)
+    assert failed == [] and set(used) == {"sq", "rect"}
+    rows = list(csv.reader(open(out / "final_result.csv")))
+    assert rows[0] == ["DataSet", "cuSparse", "spgemm", "Speedup (cuSparse / spgemm)"]
+    assert all(float(r[3]) > 0 for r in rows[1:])
+    # the rectangular product ran against the transpose and matches the oracle
+    from rtspmspm_b200 import transpose
+
+    R = read_mtx(str(d / "rect.mtx"))
+    C = read_mtx(str(out / "rect" / "result" / "spgemm.mtx"))
+    want = oracle.spgemm(R, transpose(R))
+    np.testing.assert_array_equal(C.row_ptr, want.row_ptr)
+    np.testing.assert_array_equal(C.col_idx, want.col_idx)

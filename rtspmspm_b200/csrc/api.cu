@@ -351,14 +351,18 @@ struct Pipeline {
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
         const bool use_index = ntiles > 1 && bidx_bytes <= kBlockedIndexMaxBytes && bidx_bytes < free_b / 4;
+        DevBuf tocc;
         if (use_index) {
           SPG_TRY(bidx.alloc(ctx, bidx_bytes));
+          SPG_TRY(tocc.alloc(ctx, (size_t)B.view.rows * (size_t)((ntiles + 31) / 32) * 4));
           launch_build_blocked_index(B.view, ntiles, bidx.as<int32_t>(), lc);
-          ++ctx->launches;
+          launch_build_tile_occupancy(B.view.rows, bidx.as<int32_t>(), ntiles, tocc.as<uint32_t>(), lc);
+          ctx->launches += 2;
         }
         launch_num_tile(A.view, B.view, bin_rows(kBinHeavy), nheavy, big_slot.as<int32_t>(),
                         tile_cnt.as<int32_t>(), tile_off.as<int32_t>(), ntiles, c_rp, c_col, c_val,
-                        use_index ? bidx.as<int32_t>() : nullptr, ctx->d_counter, ctx->d_flags, lc);
+                        use_index ? bidx.as<int32_t>() : nullptr, use_index ? tocc.as<uint32_t>() : nullptr,
+                        ctx->d_counter, ctx->d_flags, lc);
         ctx->launches += 2;
       }
       ++ctx->launches;

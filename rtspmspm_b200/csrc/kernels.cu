@@ -584,6 +584,26 @@ __global__ void k_build_blocked_index(DCsr B, int ntiles, int32_t* bidx) {
   }
 }
 
+// Tile occupancy of B from its blocked index: bit t of tocc[k * words + t /
+// 32] is set when B row k has an entry in column tile t.  One warp per row,
+// every word written.  ceil(tiles / 32) words per row (64 MB for 2^20 rows and
+// 512 tiles, small enough to stay in L2), so a heavy row's tile rejects the
+// rows of B that miss it with one cached load instead of four.
+__global__ void k_build_tile_occupancy(int64_t rows, const int32_t* bidx, int ntiles, int words, uint32_t* tocc) {
+  const int lane = lane_id();
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t k = gw; k < rows; k += nw) {
+    const int32_t* bi = bidx + k * (int64_t)(ntiles + 1);
+    for (int w = 0; w < words; ++w) {
+      const int t = w * 32 + lane;
+      const bool has = t < ntiles && bi[t + 1] > bi[t];
+      const unsigned m = __ballot_sync(kFull, has);
+      if (lane == 0) tocc[k * (int64_t)words + w] = m;
+    }
+  }
+}
+
 // Value-only recompute (structure of C given): per-row lengths of C and,
 // for the rows of the heavy bin, their slot and per-tile entry counts taken
 // from C's sorted columns.
@@ -661,7 +681,10 @@ __global__ void k_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const 
 
 // Segments of at least this many entries are accumulated by the whole warp
 // without collision checks; shorter ones are packed.
-constexpr int kTileLongSeg = 16;
+#ifndef SPG_TILE_LONG_SEG
+#define SPG_TILE_LONG_SEG 16
+#endif
+constexpr int kTileLongSeg = SPG_TILE_LONG_SEG;
 
 // One segment (the part of B row k inside the tile, scaled by a).  Its
 // columns are distinct, so its products need no ordering among themselves:
@@ -732,14 +755,15 @@ __device__ __forceinline__ void tile_packed(const DCsr& B, Off bs, int len, floa
     float pr[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
+      off[h] = -1 - lane;  // unique dummy for idle lanes
+      pr[h] = 0.f;
+      if (b0 + h * 32 >= total) break;  // a run of at most 32 products: one step
       const int tt = b0 + h * 32 + lane;
       const bool act = tt < total;
       const int src = warp_upper_bound(incl, act ? tt : total - 1);
       const Off sbs = __shfl_sync(kFull, bs, src);
       const int sex = __shfl_sync(kFull, excl, src);
       const float sa = __shfl_sync(kFull, a, src);
-      off[h] = -1 - lane;  // unique dummy for idle lanes
-      pr[h] = 0.f;
       if (act) {
         const Off q = sbs + (Off)(tt - sex);
         off[h] = B.col[q] - c0;
@@ -786,6 +810,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
                                                         const int32_t* big_slot, const int32_t* tile_cnt,
                                                         const int32_t* tile_off, int ntiles, const int64_t* c_rp,
                                                         int32_t* c_col, float* c_val, const int32_t* bidx,
+                                                        const uint32_t* tocc, int twords,
                                                         unsigned long long* tile_counter, int* flags) {
   using Off = typename RowOff<R32>::T;
   extern __shared__ uint32_t sm_tile[];
@@ -828,7 +853,8 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
       }
       Off bs = 0;
       int len = 0;
-      if (have) {
+      // B rows without an entry in this tile are rejected by the occupancy bit
+      if (have && (!tocc || ((tocc[(int64_t)k * twords + (tile >> 5)] >> (tile & 31)) & 1u))) {
         Off rs = RowOff<R32>::at(B, k), re = RowOff<R32>::at(B, k + 1);
         if (ntiles > 1 && re > rs) {
           // narrow to the tile's columns
@@ -1199,8 +1225,9 @@ template <bool R32>
 static void num_tile_one(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy,
                          const int32_t* big_slot, const int32_t* tile_cnt, const int32_t* tile_off, int ntiles,
                          const int64_t* c_rp, int32_t* c_col, float* c_val, const int32_t* bidx,
-                         unsigned long long* tile_counter, int* flags, const LaunchCtx& lc) {
+                         const uint32_t* tocc, unsigned long long* tile_counter, int* flags, const LaunchCtx& lc) {
   const size_t smem = (size_t)kTileWarps * (kTileCols + kTileWords + 32) * 4;
+  const int twords = (ntiles + 31) / 32;
   cudaFuncSetAttribute(k_num_tile<R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_tile<R32>, kTileWarps * 32, smem);
@@ -1209,21 +1236,27 @@ static void num_tile_one(const DCsr& A, const DCsr& B, const int32_t* heavy_rows
   const int blocks = (int)std::min<int64_t>((tiles + kTileWarps - 1) / kTileWarps, (int64_t)lc.sms * per_sm);
   cudaMemsetAsync(tile_counter, 0, sizeof(unsigned long long), lc.stream);
   k_num_tile<R32><<<blocks, kTileWarps * 32, smem, lc.stream>>>(A, B, heavy_rows, nheavy, big_slot, tile_cnt,
-                                                                tile_off, ntiles, c_rp, c_col, c_val, bidx,
-                                                                tile_counter, flags);
+                                                                tile_off, ntiles, c_rp, c_col, c_val, bidx, tocc,
+                                                                twords, tile_counter, flags);
 }
 
 void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
                      const int32_t* tile_cnt, const int32_t* tile_off, int ntiles, const int64_t* c_rp,
-                     int32_t* c_col, float* c_val, const int32_t* bidx, unsigned long long* tile_counter, int* flags,
-                     const LaunchCtx& lc) {
+                     int32_t* c_col, float* c_val, const int32_t* bidx, const uint32_t* tocc,
+                     unsigned long long* tile_counter, int* flags, const LaunchCtx& lc) {
   if (nheavy == 0) return;
   if (B.rp32)
     num_tile_one<true>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off, ntiles, c_rp, c_col, c_val, bidx,
-                       tile_counter, flags, lc);
+                       tocc, tile_counter, flags, lc);
   else
     num_tile_one<false>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off, ntiles, c_rp, c_col, c_val, bidx,
-                        tile_counter, flags, lc);
+                        tocc, tile_counter, flags, lc);
+}
+
+void launch_build_tile_occupancy(int64_t rows, const int32_t* bidx, int ntiles, uint32_t* tocc, const LaunchCtx& lc) {
+  if (rows == 0) return;
+  k_build_tile_occupancy<<<grid_for(rows, 256, 32, lc.sms * 16), 256, 0, lc.stream>>>(rows, bidx, ntiles,
+                                                                                    (ntiles + 31) / 32, tocc);
 }
 
 void launch_compact_rows(const int32_t* rows, int64_t nrows, const uint8_t* need_exact, const int64_t* slab_off,

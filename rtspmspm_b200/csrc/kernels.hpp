@@ -85,11 +85,14 @@ void launch_tile_counts_from_cols(const int32_t* heavy_rows, int64_t nheavy, con
 void launch_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot, const int32_t* tile_cnt,
                          int ntiles, int32_t* tile_off, const LaunchCtx& lc);
 void launch_build_blocked_index(const DCsr& B, int ntiles, int32_t* bidx, const LaunchCtx& lc);
-// bidx: blocked index of B (launch_build_blocked_index) or null (binary searches)
+// Tile occupancy bits of B from its blocked index (ceil(ntiles / 32) words per row).
+void launch_build_tile_occupancy(int64_t rows, const int32_t* bidx, int ntiles, uint32_t* tocc, const LaunchCtx& lc);
+// bidx: blocked index of B (launch_build_blocked_index) or null (binary
+// searches); tocc: its occupancy bits or null
 void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
                      const int32_t* tile_cnt, const int32_t* tile_off, int ntiles, const int64_t* c_rp,
-                     int32_t* c_col, float* c_val, const int32_t* bidx, unsigned long long* tile_counter, int* flags,
-                     const LaunchCtx& lc);
+                     int32_t* c_col, float* c_val, const int32_t* bidx, const uint32_t* tocc,
+                     unsigned long long* tile_counter, int* flags, const LaunchCtx& lc);
 void launch_compact_rows(const int32_t* rows, int64_t nrows, const uint8_t* need_exact, const int64_t* slab_off,
                          const int32_t* slab_col, const float* slab_val, const int64_t* c_rp, int32_t* c_col,
                          float* c_val, const LaunchCtx& lc);

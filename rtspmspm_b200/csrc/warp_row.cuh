@@ -90,33 +90,27 @@ __device__ __forceinline__ int symbolic_row(const DCsr& A, const DCsr& B, int32_
   return cnt;
 }
 
-// Records a step's new columns in the first-seen list.  Returns false when
-// LEARNED and the step overflows the capacity or the table (the learned
-// path's overflow); otherwise a full table raises kFlagHashFull.
+// Records a step's new columns in the first-seen list (at most the table's
+// size: only successful inserts are fresh).  A full table marks the lane
+// `bad` when LEARNED (the learned path's overflow, judged once at the end of
+// the row) and raises kFlagHashFull otherwise.
 template <bool LEARNED>
-__device__ __forceinline__ bool record_step(bool fresh, bool failed, int32_t j, int32_t* list, int cap, int& count,
+__device__ __forceinline__ void record_step(bool fresh, bool failed, int32_t j, int32_t* list, int& count, bool& bad,
                                             int* flags) {
   const unsigned m = __ballot_sync(kFull, fresh);
-  if (LEARNED) {
-    if (__any_sync(kFull, failed) || count + __popc(m) > cap) {
-      __syncwarp();
-      return false;
-    }
-  } else if (failed) {
-    raise_flag(flags, kFlagHashFull);
-  }
+  if (LEARNED) bad |= failed;
+  else if (failed) raise_flag(flags, kFlagHashFull);
   if (fresh) list[count + __popc(m & ((1u << lane_id()) - 1u))] = j;
   count += __popc(m);
   __syncwarp();
-  return true;
 }
 
 // One segment (B row k scaled by a), k-serial: lanes over its columns, 32 per
 // step.  Its columns are distinct, so each slot gets at most one product per
 // step and __syncwarp orders the steps.
 template <int LOGT, bool LEARNED, typename Off>
-__device__ __forceinline__ bool acc_segment(const DCsr& B, Off bs, int len, float a, int32_t* keys, float* vals,
-                                            int32_t* list, int epoch, int cap, int& count, int* flags) {
+__device__ __forceinline__ void acc_segment(const DCsr& B, Off bs, int len, float a, int32_t* keys, float* vals,
+                                            int32_t* list, int epoch, int& count, bool& bad, int* flags) {
   const int lane = lane_id();
   for (int q0 = 0; q0 < len; q0 += 32) {
     const int q = q0 + lane;
@@ -129,9 +123,8 @@ __device__ __forceinline__ bool acc_segment(const DCsr& B, Off bs, int len, floa
       if (slot < 0) failed = true;
       else vals[slot] = add_rn(fresh ? 0.f : vals[slot], pr);
     }
-    if (!record_step<LEARNED>(fresh, failed, j, list, cap, count, flags)) return false;
+    record_step<LEARNED>(fresh, failed, j, list, count, bad, flags);
   }
-  return true;
 }
 
 // Segments of lanes [lo, hi) (all shorter than kPackBelow) taken as one
@@ -141,8 +134,8 @@ __device__ __forceinline__ bool acc_segment(const DCsr& B, Off bs, int len, floa
 // the group's products in lane order, so every entry still sees its products
 // in canonical order.
 template <int LOGT, bool LEARNED, typename Off>
-__device__ __forceinline__ bool acc_packed(const DCsr& B, Off bs, int len, float a, int lo, int hi, int32_t* keys,
-                                           float* vals, int32_t* list, int epoch, int cap, int& count, int* flags) {
+__device__ __forceinline__ void acc_packed(const DCsr& B, Off bs, int len, float a, int lo, int hi, int32_t* keys,
+                                           float* vals, int32_t* list, int epoch, int& count, bool& bad, int* flags) {
   const int lane = lane_id();
   const int lr = (lane >= lo && lane < hi) ? len : 0;
   const int incl = warp_incl_scan(lr);
@@ -171,9 +164,8 @@ __device__ __forceinline__ bool acc_packed(const DCsr& B, Off bs, int len, float
     float v = (ok && !fresh) ? vals[slot] : 0.f;
     v = group_sum_in_lane_order(grp, pr, v, ok);
     if (ok) vals[slot] = v;
-    if (!record_step<LEARNED>(fresh, leader && slot < 0, j, list, cap, count, flags)) return false;
+    record_step<LEARNED>(fresh, leader && slot < 0, j, list, count, bad, flags);
   }
-  return true;
 }
 
 // Accumulates row `row` in canonical order (k ascending through A's row,
@@ -181,8 +173,9 @@ __device__ __forceinline__ bool acc_packed(const DCsr& B, Off bs, int len, float
 // a time: B rows of kPackBelow or more entries go k-serially
 // (acc_segment), runs of shorter ones are packed (acc_packed).  New columns
 // are appended to `list` in the order they are first seen; returns their
-// number, or -1 when LEARNED and more than `cap` distinct columns appear or
-// the table fills (the learned path's overflow).
+// number, or -1 when LEARNED and the row has more than `cap` distinct
+// columns or filled the table (the learned path's overflow, checked once at
+// the end of the row; the list never exceeds the table).
 template <int LOGT, bool R32, bool LEARNED>
 __device__ __forceinline__ int accumulate_row(const DCsr& A, const DCsr& B, int32_t row, int32_t* keys, float* vals,
                                               int32_t* list, int epoch, int cap, int* flags) {
@@ -190,6 +183,7 @@ __device__ __forceinline__ int accumulate_row(const DCsr& A, const DCsr& B, int3
   const int lane = lane_id();
   const int64_t s = A.rp[row], e = A.rp[row + 1];
   int count = 0;
+  bool bad = false;
   for (int64_t base = s; base < e; base += 32) {
     const int64_t p = base + lane;
     Off bs = 0;
@@ -209,17 +203,18 @@ __device__ __forceinline__ int accumulate_row(const DCsr& A, const DCsr& B, int3
         const Off sbs = __shfl_sync(kFull, bs, idx);
         const int sl = __shfl_sync(kFull, len, idx);
         const float sa = __shfl_sync(kFull, a, idx);
-        if (!acc_segment<LOGT, LEARNED>(B, sbs, sl, sa, keys, vals, list, epoch, cap, count, flags)) return -1;
+        acc_segment<LOGT, LEARNED>(B, sbs, sl, sa, keys, vals, list, epoch, count, bad, flags);
         ++idx;
       } else {
         const unsigned later = long_mask & (~0u << idx);
         const int hi = later ? min(n, __ffs(later) - 1) : n;
-        if (!acc_packed<LOGT, LEARNED>(B, bs, len, a, idx, hi, keys, vals, list, epoch, cap, count, flags))
-          return -1;
+        acc_packed<LOGT, LEARNED>(B, bs, len, a, idx, hi, keys, vals, list, epoch, count, bad, flags);
         idx = hi;
       }
     }
   }
+  // the learned capacity is judged once per row: its overflow is rare
+  if (LEARNED && (__any_sync(kFull, bad) || count > cap)) return -1;
   return count;
 }
 

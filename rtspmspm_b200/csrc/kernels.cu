@@ -124,21 +124,22 @@ __device__ __forceinline__ int bin_of(int64_t key, int64_t cols, int mode, const
 }
 
 // Histogram of bins (warp-aggregated atomics).
+// Histogram of bins: counts per block in shared memory, then one global
+// atomic per (block, bin) -- rows of one matrix mostly share a bin, so
+// per-warp global atomics would queue on one address.
 __global__ void k_bin_count(const int64_t* key, int64_t rows, int64_t cols, int mode, BinParams bp,
                             uint8_t* bin_of_row, int64_t* counts) {
-  for (int64_t r0 = blockIdx.x * (int64_t)blockDim.x; r0 < rows; r0 += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = r0 + threadIdx.x;
-    int b = -1;
-    if (r < rows) {
-      b = bin_of(key[r], cols, mode, bp);
-      bin_of_row[r] = (uint8_t)b;
-    }
-    unsigned active = __ballot_sync(kFull, r < rows);
-    if (r < rows) {
-      unsigned grp = __match_any_sync(active, b);
-      if (lane_id() == __ffs(grp) - 1) atomicAdd((unsigned long long*)&counts[b], (unsigned long long)__popc(grp));
-    }
+  __shared__ unsigned sh_cnt[kNumBins];
+  if (threadIdx.x < kNumBins) sh_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int b = bin_of(key[r], cols, mode, bp);
+    bin_of_row[r] = (uint8_t)b;
+    atomicAdd(&sh_cnt[b], 1u);
   }
+  __syncthreads();
+  if (threadIdx.x < kNumBins && sh_cnt[threadIdx.x])
+    atomicAdd((unsigned long long*)&counts[threadIdx.x], (unsigned long long)sh_cnt[threadIdx.x]);
 }
 
 // counts -> offsets[kNumBins+1]; cursors = offsets.
@@ -154,22 +155,30 @@ __global__ void k_bin_offsets(const int64_t* counts, int64_t* offsets, int64_t* 
   }
 }
 
-// Scatter row ids into per-bin lists (order within a bin follows warp
-// arrival; it only affects scheduling, never results).
+// Scatter row ids into per-bin lists: per tile of blockDim.x rows, ranks
+// inside the block from shared-memory counters, one global atomic per (tile,
+// bin) for the block's range.  Order within a bin only affects scheduling,
+// never results.
 __global__ void k_bin_scatter(const uint8_t* bin_of_row, int64_t rows, int64_t* cursors, int32_t* lists) {
+  __shared__ unsigned sh_cnt[kNumBins];
+  __shared__ unsigned long long sh_base[kNumBins];
   for (int64_t r0 = blockIdx.x * (int64_t)blockDim.x; r0 < rows; r0 += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = r0 + threadIdx.x;
-    unsigned active = __ballot_sync(kFull, r < rows);
+    if (threadIdx.x < kNumBins) sh_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t r = r0 + threadIdx.x;
+    int b = -1;
+    unsigned local = 0;
     if (r < rows) {
-      int b = bin_of_row[r];
-      unsigned grp = __match_any_sync(active, b);
-      int leader = __ffs(grp) - 1;
-      unsigned long long base = 0;
-      if (lane_id() == leader) base = atomicAdd((unsigned long long*)&cursors[b], (unsigned long long)__popc(grp));
-      base = __shfl_sync(grp, base, leader);
-      int rank = __popc(grp & ((1u << lane_id()) - 1u));
-      lists[base + rank] = (int32_t)r;
+      b = bin_of_row[r];
+      local = atomicAdd(&sh_cnt[b], 1u);
     }
+    __syncthreads();
+    if (threadIdx.x < kNumBins && sh_cnt[threadIdx.x])
+      sh_base[threadIdx.x] = atomicAdd((unsigned long long*)&cursors[threadIdx.x],
+                                       (unsigned long long)sh_cnt[threadIdx.x]);
+    __syncthreads();
+    if (b >= 0) lists[sh_base[b] + local] = (int32_t)r;
+    __syncthreads();
   }
 }
 
@@ -230,6 +239,35 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int64_t* in, 
     if (base + i < n) out[base + i] = pre;
     pre += v[i];
   }
+}
+
+// Second pass of the two-kernel scan (at most kScanTile blocks): each block
+// sums the block totals before it, scans its tile on top, and the last block
+// also writes the grand total to out[n].  out may alias in.
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply_sums(const int64_t* in, int64_t n, const int64_t* sums,
+                                                                    int64_t* out) {
+  __shared__ int64_t sh[33];
+  // prefix of the block sums before this block
+  int64_t ps = 0;
+  for (int64_t i = threadIdx.x; i < blockIdx.x; i += blockDim.x) ps += sums[i];
+  int64_t tot_before;
+  block_excl_scan(ps, sh, tot_before);
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int64_t v[kScanItems];
+  int64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    v[i] = (base + i < n) ? in[base + i] : 0;
+    s += v[i];
+  }
+  int64_t tot;
+  int64_t pre = block_excl_scan(s, sh, tot) + tot_before;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i < n) out[base + i] = pre;
+    pre += v[i];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = tot_before + tot;
 }
 
 __global__ void k_store_total(const int64_t* excl_last, const int64_t* in_last, int64_t* dst) {
@@ -1013,6 +1051,13 @@ void launch_excl_scan(const int64_t* in, int64_t n, int64_t* out, int64_t* tmp, 
     return;
   }
   const int64_t nb = (n + kScanTile - 1) / kScanTile;
+  if (nb <= kScanTile) {
+    // two kernels: block totals, then each block adds the totals before it
+    int64_t* sums = tmp + 1;
+    k_scan_reduce<<<(unsigned)nb, kScanThreads, 0, lc.stream>>>(in, n, sums);
+    k_scan_apply_sums<<<(unsigned)nb, kScanThreads, 0, lc.stream>>>(in, n, sums, out);
+    return;
+  }
   // keep the last input element so out may alias in
   int64_t* last = tmp;
   cudaMemcpyAsync(last, in + n - 1, sizeof(int64_t), cudaMemcpyDeviceToDevice, lc.stream);

@@ -43,6 +43,26 @@ def test_tensor_core_inference_matches_reference(engine):
     np.testing.assert_allclose(y, ry, rtol=2e-2, atol=2e-2)
 
 
+@pytest.mark.parametrize("bits", [32, 64])
+def test_features_match_oracle(engine, bits):
+    """The feature kernel's integer statistics and features equal the CPU
+    restatement: short and long rows (> 32 entries, sampled by stride),
+    empty rows and columns, a heavy row, rectangular shapes, a ragged last
+    tile, and both row-pointer widths."""
+    from cases import heavy_row, with_empty_rows_cols
+
+    mats = [(gen.stencil27(10, seed=1), None), (gen.rmat(12, 16, seed=5), None),
+            (gen.erdos_renyi(333, 250, 7.0, 2), gen.erdos_renyi(250, 517, 40.0, 3)),
+            (with_empty_rows_cols(), None), (heavy_row(), None), (gen.erdos_renyi(17, 17, 0.5, 4), None)]
+    for A, B in mats:
+        B = A if B is None else B
+        dA, dB = DeviceCsr.from_host(A, index_bits=bits), DeviceCsr.from_host(B, index_bits=bits)
+        got = engine.features(dA, dB).cpu().numpy()
+        ref, _ = mlp_oracle.row_features(A, B)
+        # integer features exactly (up to log2f's rounding), float ones to 2 ulp
+        np.testing.assert_allclose(got, ref, rtol=0, atol=5e-7)
+
+
 def test_training_reduces_loss_and_roundtrips(tmp_path):
     eng = Engine(0)
     try:

@@ -326,22 +326,27 @@ __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B
   __shared__ MlpSmem sm;
   __shared__ float tile[kPlanWarps][16 * kMlpIn];
   __shared__ int64_t tprod[kPlanWarps][16];
+  __shared__ RowStats tstat[kPlanWarps][16];
   load_mlp_smem(w, sm);
   const int lane = lane_id(), wib = threadIdx.x >> 5;
   const int64_t rows = A.rows;
   const int64_t ntiles = (rows + 15) / 16;
   for (int64_t t = blockIdx.x * (int64_t)kPlanWarps + wib; t < ntiles; t += (int64_t)gridDim.x * kPlanWarps) {
     const int64_t r0 = t * 16;
-    for (int i = 0; i < 16; ++i) {
-      const int64_t r = r0 + i;
-      if (r < rows) {
-        const RowStats st = row_stats<R32>(A, B, r);
-        if (lane < kMlpIn) tile[wib][i * kMlpIn + lane] = feature_of(st, B.cols, lane);
-        if (lane == 0) tprod[wib][i] = st.sum;
-      } else {
-        if (lane < kMlpIn) tile[wib][i * kMlpIn + lane] = 0.f;
-        if (lane == 0) tprod[wib][i] = 0;
+    const int nr = rows - r0 < 16 ? (int)(rows - r0) : 16;
+    for (int i = 0; i < nr; ++i) {
+      const RowStats st = row_stats<R32>(A, B, r0 + i);
+      if (lane == 0) {
+        tstat[wib][i] = st;
+        tprod[wib][i] = st.sum;
       }
+    }
+    if (lane >= nr && lane < 16) tprod[wib][lane] = 0;
+    __syncwarp();
+    // the tile's 128 features, four per lane
+    for (int idx = lane; idx < 16 * kMlpIn; idx += 32) {
+      const int i = idx / kMlpIn;
+      tile[wib][idx] = i < nr ? feature_of(tstat[wib][i], B.cols, idx % kMlpIn) : 0.f;
     }
     __syncwarp();
     float o[4];

@@ -134,11 +134,24 @@ def cpu_sample(A, target_s: float, threads: int | None = None):
     want = min(float(cum[-1]), rate * target_s)
     r2 = int(np.searchsorted(cum, want)) + 1
     r2 = min(r2, A.rows)
+    # a workload shorter than the target is run whole, pass after pass,
+    # until the target time is filled
+    passes = 0
     t = time.perf_counter()
-    oracle.baseline_rows(A, A, 0, r2)
-    dt = time.perf_counter() - t
-    work = float(cum[r2 - 1])
-    return 2.0 * work / dt / 1e9, {"cores": cores, "rows": r2, "products": int(work), "seconds": dt}
+    while True:
+        oracle.baseline_rows(A, A, 0, r2)
+        passes += 1
+        dt = time.perf_counter() - t
+        if r2 < A.rows or dt >= target_s:
+            break
+    work = float(cum[r2 - 1]) * passes
+    return 2.0 * work / dt / 1e9, {"cores": cores, "rows": r2, "products": int(work), "seconds": dt,
+                                   "passes": passes}
+
+
+def sample_text(info, what: str) -> str:
+    head = f"{info['passes']} passes over all" if info["passes"] > 1 else "leading"
+    return f"{head} {info['rows']} rows of {what} ({info['products']} products, {info['seconds']:.1f} s)"
 
 
 def reference_arm(args, A):
@@ -153,11 +166,11 @@ def reference_arm(args, A):
         if i >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
-    sample = f"leading {info['rows']} rows of the stencil-96 C=A*A ({info['products']} products, " \
-             f"{info['seconds']:.1f} s per step)"
+    sample = f"{sample_text(info, 'the stencil-96 C=A*A')} per step"
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GFLOP/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(info["seconds"] * 1e3, 3),
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(info["seconds"] / info["passes"] * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "sample": "bounded row sample"},
         "cpu_baseline": {"value": round(value, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
@@ -255,8 +268,7 @@ def other_workload(args) -> int:
         if args.workload == "rmat20" and not args.no_cpu:
             v, info = cpu_sample(A, args.cpu_seconds)
             out["cpu_baseline"] = {"value": round(v, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
-                                   "sample": f"leading {info['rows']} rows ({info['products']} products, "
-                                             f"{info['seconds']:.1f} s)"}
+                                   "sample": sample_text(info, "the same C=A*A")}
     print(json.dumps(out), flush=True)
     eng.close()
     return 0
@@ -454,8 +466,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         v, info = cpu_sample(A, args.cpu_seconds)
         cpu = {"value": round(v, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
-               "sample": f"leading {info['rows']} rows of the same C=A*A ({info['products']} products, "
-                         f"{info['seconds']:.1f} s)"}
+               "sample": sample_text(info, "the same C=A*A")}
 
     value = world * flops / (ms_learned * 1e-3) / 1e9
     line = {

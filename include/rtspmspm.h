@@ -337,7 +337,8 @@ spg_status spg_mlp_grad(spg_ctx* ctx, const float* d_features, const float* d_ta
 
 typedef struct spg_tuning {
     int32_t warp_table_max;    /* largest per-warp hash table (entries) */
-    int32_t warps_per_block;   /* warps per CTA for the warp-hash bins */
+    int32_t warps_per_block;   /* warps per CTA for the warp-hash bins; 0 (default):
+                                  per kernel, the size with the most resident warps */
     float   max_load;          /* hash-table load factor used for sizing */
     int32_t tile_cols;         /* column width of a heavy-row tile (power of two) */
     int32_t block_table_max;   /* CTA hash table for the symbolic mid bin */

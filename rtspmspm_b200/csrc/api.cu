@@ -62,10 +62,10 @@ void DevBuf::reset() {
 spg_tuning default_tuning() {
   spg_tuning t{};
   t.warp_table_max = 4096;
-  // 4-warp CTAs: stencil 96^3 learned numeric 4.18 -> 3.81 ms against 8-warp
-  // CTAs (the 2^9-slot tables take 6 KB per warp, so smaller CTAs pack the
-  // SM's shared memory more finely); plain 7.43 -> 7.38 ms
-  t.warps_per_block = 4;
+  // 0: each warp-hash kernel takes the CTA size with the most resident warps
+  // per SM (fixed 8-warp CTAs left the stencil 96^3 numeric kernels at 32
+  // warps per SM instead of 36: learned numeric 4.18 ms against 3.79 ms)
+  t.warps_per_block = 0;
   t.max_load = 0.4f;  // measured best for the plain method on the stencil rows (0.3..0.65 swept)
   t.tile_cols = kTileCols;
   t.block_table_max = 16384;
@@ -257,7 +257,7 @@ struct Pipeline {
   Pipeline(spg_ctx* c, const DevMat& a, const DevMat& b, const spg_tuning& t)
       : ctx(c), lc(launch_ctx(c)), A(a), B(b), tune(t), bp(bin_params(t)), rows(a.view.rows), cols(b.view.cols) {
     ntiles = (int)std::max<int64_t>(1, (cols + kTileCols - 1) / kTileCols);
-    wpb = std::max(1, std::min(16, t.warps_per_block));
+    wpb = t.warps_per_block <= 0 ? 0 : std::min(16, t.warps_per_block);
   }
 
   int64_t* counts() { return binmeta.as<int64_t>(); }

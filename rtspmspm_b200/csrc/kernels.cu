@@ -13,6 +13,8 @@
 //       instead of a dense rows x cols buffer (optixSpMSpM.cpp:164-171).
 //   compaction + per-row sort -- the dense-to-COO scan of printResult
 //       (optixSpMSpM.cpp:452-494), done per row on the device.
+#include <atomic>
+
 #include "common.cuh"
 #include "kernels.hpp"
 #include "tile.cuh"
@@ -1072,11 +1074,56 @@ void launch_excl_scan(const int64_t* in, int64_t n, int64_t* out, int64_t* tmp, 
   k_store_total<<<1, 32, 0, lc.stream>>>(out + n - 1, last, out + n);
 }
 
+static int wpb_for(int log_t, int wpb) {
+  // keep a CTA's tables within 96 KB
+  const int per_warp = (1 << log_t) * 12;
+  int lim = (96 * 1024) / per_warp;
+  if (lim < 1) lim = 1;
+  return std::max(1, std::min(wpb, lim));
+}
+
+// CTA size (warps, 1..max_w) giving a kernel the most resident warps per SM
+// for `smem_per_warp` bytes of dynamic shared memory per warp; ties go to
+// the larger CTA.  Register and shared-memory granularity make this differ
+// by table size: 2^9-slot numeric tables (6 KB a warp) reach 36 warps with
+// 6-warp CTAs but 32 with 8-warp ones; 2^11-slot symbolic tables (8 KB) fit
+// 28 warps with 7-warp CTAs and 24 with 8-warp ones.
+template <typename Kernel>
+static int auto_wpb(Kernel kernel, size_t smem_per_warp, int max_w) {
+  int best_w = 1, best = -1;
+  for (int w = 1; w <= max_w; ++w) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, w * 32, (size_t)w * smem_per_warp) !=
+        cudaSuccess)
+      continue;
+    if (per_sm * w >= best) {
+      best = per_sm * w;
+      best_w = w;
+    }
+  }
+  return best_w;
+}
+
+// wpb <= 0 selects auto_wpb, computed once per kernel instantiation (the
+// first device that launches it decides; all devices here are alike).
+template <typename Kernel>
+static int resolve_wpb(int wpb, std::atomic<int>& cache, Kernel kernel, size_t smem_per_warp, int max_w) {
+  if (wpb > 0) return wpb;
+  int w = cache.load(std::memory_order_relaxed);
+  if (w <= 0) {
+    w = auto_wpb(kernel, smem_per_warp, max_w);
+    cache.store(w, std::memory_order_relaxed);
+  }
+  return w;
+}
+
 template <int LOGT, bool R32>
 static void sym_warp_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int64_t* nnz, int* flags,
                          const LaunchCtx& lc, int wpb) {
-  const size_t smem = (size_t)wpb * (1 << LOGT) * sizeof(int32_t);
   cudaFuncSetAttribute(k_sym_warp<LOGT, R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  static std::atomic<int> auto_w{0};
+  wpb = resolve_wpb(wpb, auto_w, k_sym_warp<LOGT, R32>, (size_t)(1 << LOGT) * sizeof(int32_t), 8);
+  const size_t smem = (size_t)wpb * (1 << LOGT) * sizeof(int32_t);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sym_warp<LOGT, R32>, wpb * 32, smem);
   if (per_sm < 1) per_sm = 1;
@@ -1087,7 +1134,7 @@ static void sym_warp_one(const DCsr& A, const DCsr& B, const int32_t* rows, int6
 void launch_sym_warp(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int64_t* nnz,
                      int* flags, const LaunchCtx& lc, int wpb) {
   if (nrows == 0) return;
-  const int w = log_t >= 11 ? std::min(wpb, 8) : wpb;
+  const int w = wpb <= 0 ? 0 : log_t >= 11 ? std::min(wpb, 8) : wpb;
 #define SPG_SW(L)                                                                   \
   case L:                                                                           \
     if (B.rp32) sym_warp_one<L, true>(A, B, rows, nrows, nnz, flags, lc, w);        \
@@ -1145,8 +1192,10 @@ void launch_sym_dense(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t
 template <int LOGT, bool R32>
 static void num_warp_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, const int64_t* c_rp,
                          int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb) {
-  const size_t smem = (size_t)wpb * numeric_words<LOGT>() * 4;
   cudaFuncSetAttribute(k_num_warp<LOGT, R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  static std::atomic<int> auto_w{0};
+  wpb = resolve_wpb(wpb, auto_w, k_num_warp<LOGT, R32>, (size_t)numeric_words<LOGT>() * 4, wpb_for(LOGT, 8));
+  const size_t smem = (size_t)wpb * numeric_words<LOGT>() * 4;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_warp<LOGT, R32>, wpb * 32, smem);
   if (per_sm < 1) per_sm = 1;
@@ -1154,18 +1203,10 @@ static void num_warp_one(const DCsr& A, const DCsr& B, const int32_t* rows, int6
   k_num_warp<LOGT, R32><<<blocks, wpb * 32, smem, lc.stream>>>(A, B, rows, nrows, c_rp, c_col, c_val, flags);
 }
 
-static int wpb_for(int log_t, int wpb) {
-  // keep a CTA's tables within 96 KB
-  const int per_warp = (1 << log_t) * 12;
-  int lim = (96 * 1024) / per_warp;
-  if (lim < 1) lim = 1;
-  return std::max(1, std::min(wpb, lim));
-}
-
 void launch_num_warp(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
                      const int64_t* c_rp, int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb) {
   if (nrows == 0) return;
-  const int w = wpb_for(log_t, wpb);
+  const int w = wpb <= 0 ? 0 : wpb_for(log_t, wpb);
 #define SPG_NW(L)                                                                          \
   case L:                                                                                  \
     if (B.rp32) num_warp_one<L, true>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); \
@@ -1183,8 +1224,11 @@ static void num_warp_learned_one(const DCsr& A, const DCsr& B, const int32_t* ro
                                  const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
                                  int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
                                  const LaunchCtx& lc, int wpb) {
-  const size_t smem = (size_t)wpb * numeric_words<LOGT>() * 4;
   cudaFuncSetAttribute(k_num_warp_learned<LOGT, R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  static std::atomic<int> auto_w{0};
+  wpb = resolve_wpb(wpb, auto_w, k_num_warp_learned<LOGT, R32>, (size_t)numeric_words<LOGT>() * 4,
+                    wpb_for(LOGT, 8));
+  const size_t smem = (size_t)wpb * numeric_words<LOGT>() * 4;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_warp_learned<LOGT, R32>, wpb * 32, smem);
   if (per_sm < 1) per_sm = 1;
@@ -1199,7 +1243,7 @@ void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int3
                              int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
                              const LaunchCtx& lc, int wpb) {
   if (nrows == 0) return;
-  const int w = wpb_for(log_t, wpb);
+  const int w = wpb <= 0 ? 0 : wpb_for(log_t, wpb);
 #define SPG_NWL(L)                                                                                             \
   case L:                                                                                                      \
     if (B.rp32)                                                                                                \

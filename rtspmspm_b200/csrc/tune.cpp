@@ -123,7 +123,8 @@ spg_status spg_set_tuning(spg_ctx* ctx, const spg_tuning* in) {
   if (t.warp_table_max < 32 || t.warp_table_max > 4096 || (t.warp_table_max & (t.warp_table_max - 1)))
     return fail(ctx, SPG_ERR_INVALID_ARG, "warp_table_max must be a power of two in [32, 4096]");
   if (!(t.max_load > 0.05f && t.max_load < 0.95f)) return fail(ctx, SPG_ERR_INVALID_ARG, "max_load out of range");
-  if (t.warps_per_block < 1 || t.warps_per_block > 16) return fail(ctx, SPG_ERR_INVALID_ARG, "warps_per_block 1..16");
+  if (t.warps_per_block < 0 || t.warps_per_block > 16)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "warps_per_block 0 (per kernel) or 1..16");
   if (t.block_table_max < 1024 || t.block_table_max > 32768 || (t.block_table_max & (t.block_table_max - 1)))
     return fail(ctx, SPG_ERR_INVALID_ARG, "block_table_max must be a power of two in [1024, 32768]");
   if (t.tile_cols == 0) t.tile_cols = d.tile_cols;
@@ -154,7 +155,7 @@ spg_status spg_tune(spg_ctx* ctx, int32_t n, const spg_csr* A, const spg_csr* B,
   // single product searches the largest table
   const std::vector<int> tables = n > 1 ? std::vector<int>{4096} : std::vector<int>{1024, 2048, 4096};
   const float loads[] = {0.35f, 0.5f, 0.65f};
-  const int wpbs[] = {4, 8, 16};
+  const int wpbs[] = {0, 4, 8, 16};
   const int blocks[] = {8192, 16384};
   for (int wt : tables)
     for (float ld : loads)

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle
-from rtspmspm_b200 import DeviceCsr, gen
+from rtspmspm_b200 import DeviceCsr, SpgError, gen
 
 from cases import named_pairs
 from helpers import assert_parity, assert_same_structure, value_errors, REL_TOL
@@ -47,6 +47,20 @@ def test_parity(engine, name, A, B, algo, tuning):
     assert rep["nnz_c"] == R.nnz
     assert rep["products"] == int(gen.row_products(A, B).sum())
     assert rep["device_flags"] == 0
+
+
+@pytest.mark.parametrize("wpb", [0, 1, 3, 6])
+@pytest.mark.parametrize("algo", ["plain", "learned"])
+def test_cta_sizes(engine, algo, wpb):
+    """Per-kernel CTA sizes (0) and odd explicit ones give the same C."""
+    engine.set_tuning(warps_per_block=wpb)
+    for name, A, B in PAIRS:
+        if name in ("stencil12", "rmat12", "er4096", "rect"):
+            C, rep = engine.multiply(A, B, algo=algo, use_tuning=True)
+            assert_parity(C.to_host(), ref(name, A, B))
+    for bad in (-1, 17):
+        with pytest.raises(SpgError):
+            engine.set_tuning(warps_per_block=bad)
 
 
 @pytest.mark.parametrize("name,A,B", PAIRS[:9], ids=[p[0] for p in PAIRS[:9]])

@@ -37,9 +37,9 @@ struct BatchMat {
   int64_t rp_base;    // first entry of C_m's row pointers in the row-pointer slab
 };
 
-// Warps per CTA of the per-bin kernels; a CTA's tables stay within 96 KB.
+// Largest CTA of the per-bin kernels: 8 warps, tables within 200 KB.
 constexpr int kBatchWarps = 8;
-constexpr int kBatchCtaTableBytes = 96 * 1024;
+constexpr int kBatchCtaTableBytes = 200 * 1024;
 
 // Products per global row and the bound min(products, cols_m).
 __global__ void k_batch_products(const BatchMat* mats, const int32_t* row_mat, int64_t R, int64_t* prod,
@@ -77,12 +77,9 @@ __global__ void k_batch_bound_stats(const int32_t* row_mat, const int64_t* bound
   }
 }
 
-// Warps per CTA for tables of 2^logt slots (keys only when symbolic; keys,
-// values and first-seen list when numeric).
-inline int batch_warps(int logt, bool numeric) {
-  const int per_warp = (1 << logt) * (numeric ? 12 : 4);
-  return std::max(1, std::min(kBatchWarps, kBatchCtaTableBytes / per_warp));
-}
+// Shared-memory bytes a warp's table takes: 2^logt slots of keys when
+// symbolic; keys, values and the first-seen list when numeric.
+inline size_t batch_table_bytes(int logt, bool numeric) { return ((size_t)1 << logt) * (numeric ? 12 : 4); }
 
 // Symbolic (NUMERIC = false) or numeric (true) pass over the rows of warp
 // bin LOGT of the global row space: warp per row, rows taken in stride from
@@ -190,6 +187,7 @@ struct BatchPlan {
   cudaGraph_t graph = nullptr;
   spg_tuning tune{};
   int per_sm[2][kNumWarpBins] = {};  // CTAs per SM of the per-bin kernels (symbolic, numeric)
+  int warps[2][kNumWarpBins] = {};   // warps per CTA of the per-bin kernels
   int launches = 0;
 };
 
@@ -255,8 +253,8 @@ void enqueue(spg_ctx* ctx, BatchPlan* p) {
   auto stage = [&](bool numeric) {
     for (int b = 0; b < kNumWarpBins; ++b) {
       const int logt = kMinLogT + b;
-      const int w = batch_warps(logt, numeric);
-      const size_t smem = (size_t)w * (numeric ? 3 : 1) * ((size_t)1 << logt) * 4;
+      const int w = p->warps[numeric ? 1 : 0][b];
+      const size_t smem = (size_t)w * batch_table_bytes(logt, numeric);
       const int grid = lc.sms * p->per_sm[numeric ? 1 : 0][b];
 #define SPG_BB(L)                                                                                                 \
   case L:                                                                                                         \
@@ -420,31 +418,44 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
   SPG_CUDA(ctx, cudaMemcpyAsync(p->d_mats, p->mats.data(), (size_t)n * sizeof(BatchMat), cudaMemcpyHostToDevice,
                                 ctx->stream));
   SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  // shared memory and CTAs per SM of every per-bin kernel (set before any capture)
+  // CTA size, shared memory and CTAs per SM of every per-bin kernel (set
+  // before any capture): of 1..kBatchWarps warps whose tables fit
+  // kBatchCtaTableBytes, the size with the most resident warps per SM, ties
+  // to the larger CTA
   for (int numeric = 0; numeric < 2; ++numeric) {
     for (int b = 0; b < kNumWarpBins; ++b) {
       const int logt = kMinLogT + b;
-      const int w = batch_warps(logt, numeric != 0);
-      const size_t smem = (size_t)w * (numeric ? 3 : 1) * ((size_t)1 << logt) * 4;
-      int per_sm = 0;
-#define SPG_BA(L)                                                                                             \
-  case L:                                                                                                     \
-    if (numeric) {                                                                                            \
-      SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_bin<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                                         (int)smem));                                                         \
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_bin<L, true>, w * 32, smem);             \
-    } else {                                                                                                  \
-      SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_bin<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                         (int)smem));                                                         \
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_bin<L, false>, w * 32, smem);            \
-    }                                                                                                         \
+      const size_t per_warp = batch_table_bytes(logt, numeric != 0);
+      const int max_w = (int)std::max<size_t>(1, std::min<size_t>(kBatchWarps, kBatchCtaTableBytes / per_warp));
+      int best_w = 1, best_ctas = 1, best = -1;
+      for (int w = 1; w <= max_w; ++w) {
+        const size_t smem = (size_t)w * per_warp;
+        int per_sm = 0;
+#define SPG_BA(L)                                                                                            \
+  case L:                                                                                                    \
+    if (numeric) {                                                                                           \
+      SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_bin<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                         (int)kBatchCtaTableBytes));                                         \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_bin<L, true>, w * 32, smem);            \
+    } else {                                                                                                 \
+      SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_bin<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                         (int)kBatchCtaTableBytes));                                         \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_bin<L, false>, w * 32, smem);           \
+    }                                                                                                        \
     break;
-      switch (logt) {
-        SPG_BA(5) SPG_BA(6) SPG_BA(7) SPG_BA(8) SPG_BA(9) SPG_BA(10) SPG_BA(11) SPG_BA(12)
-        default: break;
-      }
+        switch (logt) {
+          SPG_BA(5) SPG_BA(6) SPG_BA(7) SPG_BA(8) SPG_BA(9) SPG_BA(10) SPG_BA(11) SPG_BA(12)
+          default: break;
+        }
 #undef SPG_BA
-      p->per_sm[numeric][b] = std::max(1, per_sm);
+        if (per_sm >= 1 && per_sm * w >= best) {
+          best = per_sm * w;
+          best_w = w;
+          best_ctas = per_sm;
+        }
+      }
+      p->warps[numeric][b] = best_w;
+      p->per_sm[numeric][b] = best_ctas;
     }
   }
   SPG_TRY(dmalloc(ctx, p, &p->nnz, (size_t)R + 1));

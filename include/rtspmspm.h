@@ -68,7 +68,7 @@ typedef struct spg_csr {
     int32_t  reserved;
 } spg_csr;
 
-#define SPG_ALGO_PLAIN     0  /* symbolic pass + numeric pass (the judge / fallback) */
+#define SPG_ALGO_PLAIN     0  /* symbolic pass + numeric pass (exact sizes; the fallback) */
 #define SPG_ALGO_LEARNED   1  /* MLP-sized single numeric pass, overflow -> exact re-run */
 #define SPG_ALGO_CUSPARSE  2  /* cusparseSpGEMM ALG3, reported reference point only */
 

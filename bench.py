@@ -151,6 +151,29 @@ def cpu_sample(A, target_s: float, threads: int | None = None):
                                    "passes": passes}
 
 
+def scipy_sample(A, target_s: float):
+    """scipy.sparse A[:r] @ A (single-threaded SMMP, FP32 CSR) on the leading
+    rows of the product, sized to about target_s seconds: a second CPU
+    reference beside the oracle.  Returns (GFLOP/s, rows, seconds) or None."""
+    try:
+        import scipy.sparse as sp
+    except ImportError:
+        return None
+    from rtspmspm_b200 import gen
+
+    S = sp.csr_matrix((A.val, A.col_idx, A.row_ptr), shape=(A.rows, A.cols))
+    cum = np.cumsum(gen.row_products(A, A))
+    r1 = int(np.searchsorted(cum, cum[-1] * 0.002)) + 1
+    t = time.perf_counter()
+    S[:r1] @ S
+    rate = float(cum[r1 - 1]) / max(time.perf_counter() - t, 1e-4)
+    r2 = min(A.rows, int(np.searchsorted(cum, min(float(cum[-1]), rate * target_s))) + 1)
+    t = time.perf_counter()
+    S[:r2] @ S
+    dt = time.perf_counter() - t
+    return 2.0 * float(cum[r2 - 1]) / dt / 1e9, r2, dt
+
+
 def sample_text(info, what: str) -> str:
     head = f"{info['passes']} passes over all" if info["passes"] > 1 else "leading"
     return f"{head} {info['rows']} rows of {what} ({info['products']} products, {info['seconds']:.1f} s)"
@@ -465,10 +488,15 @@ def main():
                 "whole_call_frac": round(bytes_alg / (ms_learned * 1e-3) / 1e9 / peak, 4)}
 
     cpu = None
+    cpu_scipy = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, info = cpu_sample(A, args.cpu_seconds)
         cpu = {"value": round(v, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
                "sample": sample_text(info, "the same C=A*A")}
+        sc = scipy_sample(A, 5.0)
+        if sc is not None:
+            cpu_scipy = {"value": round(sc[0], 4), "unit": "GFLOP/s", "threads": 1,
+                         "sample": f"scipy.sparse A[:{sc[1]}] @ A ({sc[2]:.1f} s)"}
 
     value = world * flops / (ms_learned * 1e-3) / 1e9
     line = {
@@ -488,6 +516,7 @@ def main():
         "reuse": reuse,
         "roofline": roofline,
         "cpu_baseline": cpu,
+        "cpu_scipy": cpu_scipy,
         "e2e": {"value": round(world * flops / (e2e_ms_step * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
                 "ms_per_step": round(e2e_ms_step, 4), "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "call": f"spg_multiply_into_host, {args.e2e_blocks} row blocks"},

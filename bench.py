@@ -174,6 +174,32 @@ def scipy_sample(A, target_s: float):
     return 2.0 * float(cum[r2 - 1]) / dt / 1e9, r2, dt
 
 
+def parity_sample(A, c_rp, c_col, c_val, lo: int, hi: int) -> dict:
+    """Rows lo..hi-1 of the engine's C = A*A (host arrays) against the oracle
+    (the checker): structure, bit equality with the FP32 canonical oracle,
+    the error relative to sum|a*b| and the error against the FP64 twin."""
+    from oracle import oracle
+    from rtspmspm_b200.gen import Csr
+
+    s0, s1 = int(A.row_ptr[lo]), int(A.row_ptr[hi])
+    sub = Csr(hi - lo, A.cols, np.asarray(A.row_ptr[lo:hi + 1], np.int64) - s0, A.col_idx[s0:s1], A.val[s0:s1])
+    R = oracle.spgemm(sub, A)
+    c0, c1 = int(c_rp[lo]), int(c_rp[hi])
+    rp = np.asarray(c_rp[lo:hi + 1], np.int64) - c0
+    col, val = np.asarray(c_col[c0:c1]), np.asarray(c_val[c0:c1], np.float32)
+    same = bool(np.array_equal(rp, R.row_ptr) and np.array_equal(col, R.col_idx))
+    out = {"rows": f"{lo}..{hi - 1}", "nnz": int(c1 - c0), "structure_exact": same}
+    if same:
+        v = val.astype(np.float64)
+        rel = np.abs(v - R.val.astype(np.float64)) / np.maximum(R.bound, np.finfo(np.float64).tiny)
+        e64 = np.abs(v - R.val64)
+        out.update({"bit_exact_fp32": bool(np.array_equal(val.view(np.uint32), R.val.view(np.uint32))),
+                    "max_rel_err_vs_sum_abs": float(rel.max()) if rel.size else 0.0,
+                    "max_abs_err_fp64": float(e64.max()) if e64.size else 0.0,
+                    "mean_abs_err_fp64": float(e64.mean()) if e64.size else 0.0})
+    return out
+
+
 def sample_text(info, what: str) -> str:
     head = f"{info['passes']} passes over all" if info["passes"] > 1 else "leading"
     return f"{head} {info['rows']} rows of {what} ({info['products']} products, {info['seconds']:.1f} s)"
@@ -489,10 +515,14 @@ def main():
 
     cpu = None
     cpu_scipy = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, info = cpu_sample(A, args.cpu_seconds)
         cpu = {"value": round(v, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
                "sample": sample_text(info, "the same C=A*A")}
+        mid = A.rows // 2
+        parity = parity_sample(A, host_c[0].numpy(), host_c[1].numpy(), host_c[2].numpy(), mid,
+                               min(A.rows, mid + 4096))
         sc = scipy_sample(A, 5.0)
         if sc is not None:
             cpu_scipy = {"value": round(sc[0], 4), "unit": "GFLOP/s", "threads": 1,
@@ -517,6 +547,7 @@ def main():
         "roofline": roofline,
         "cpu_baseline": cpu,
         "cpu_scipy": cpu_scipy,
+        "parity_sample": parity,
         "e2e": {"value": round(world * flops / (e2e_ms_step * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
                 "ms_per_step": round(e2e_ms_step, 4), "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "call": f"spg_multiply_into_host, {args.e2e_blocks} row blocks"},

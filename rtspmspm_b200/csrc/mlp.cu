@@ -313,8 +313,9 @@ __device__ __forceinline__ void capacity_of(int64_t p, int64_t cols, float o0, f
   cap = c;
 }
 
-// Learned plan: per 16-row tile, the warp computes each row's features and
-// products, runs the MLP on the tile with tensor cores, and writes the
+// Learned plan: per 16-row tile, the warp gathers each row's statistics
+// (row by row, the whole warp on a row), computes the tile's 128 features
+// four per lane, runs the MLP on the tile with tensor cores, and writes the
 // products, capacity and exact-path mark of every row; n_exact counts the
 // rows marked for the exact path.
 template <bool R32>

@@ -90,19 +90,37 @@ __device__ __forceinline__ int symbolic_row(const DCsr& A, const DCsr& B, int32_
   return cnt;
 }
 
-// Records a step's new columns in the first-seen list (at most the table's
-// size: only successful inserts are fresh).  A full table marks the lane
-// `bad` when LEARNED (the learned path's overflow, judged once at the end of
-// the row) and raises kFlagHashFull otherwise.
+// Ends a step: a full table marks the lane `bad` when LEARNED (the learned
+// path's overflow, judged once at the end of the row) and raises
+// kFlagHashFull otherwise; __syncwarp orders the steps.
 template <bool LEARNED>
-__device__ __forceinline__ void record_step(bool fresh, bool failed, int32_t j, int32_t* list, int& count, bool& bad,
-                                            int* flags) {
-  const unsigned m = __ballot_sync(kFull, fresh);
+__device__ __forceinline__ void end_step(bool failed, bool& bad, int* flags) {
   if (LEARNED) bad |= failed;
   else if (failed) raise_flag(flags, kFlagHashFull);
-  if (fresh) list[count + __popc(m & ((1u << lane_id()) - 1u))] = j;
-  count += __popc(m);
   __syncwarp();
+}
+
+// Gathers the row's columns from its table into `list` (slot order; the
+// emitters sort them) and returns their number.  A slot is live when its key
+// carries the row's epoch (epoch-tagged tables) or is not empty (plain keys).
+// One pass of T / 32 reads per lane replaces a per-step record of new
+// columns; the table holds at most T keys, so the list does too.
+template <int LOGT>
+__device__ __forceinline__ int gather_columns(const int32_t* keys, int32_t* list, int epoch) {
+  constexpr int T = 1 << LOGT;
+  const int lane = lane_id();
+  const unsigned lt = (1u << lane) - 1u;
+  int count = 0;
+#pragma unroll 4
+  for (int s0 = 0; s0 < T; s0 += 32) {
+    const int32_t k = keys[s0 + lane];
+    const bool live = epoch >= 0 ? ((uint32_t)k >> 24) == (uint32_t)epoch : k != kEmpty;
+    const unsigned m = __ballot_sync(kFull, live);
+    if (live) list[count + __popc(m & lt)] = epoch >= 0 ? (int32_t)((uint32_t)k & 0xFFFFFFu) : k;
+    count += __popc(m);
+  }
+  __syncwarp();
+  return count;
 }
 
 // One segment (B row k scaled by a), k-serial: lanes over its columns, 32 per
@@ -110,20 +128,20 @@ __device__ __forceinline__ void record_step(bool fresh, bool failed, int32_t j, 
 // step and __syncwarp orders the steps.
 template <int LOGT, bool LEARNED, typename Off>
 __device__ __forceinline__ void acc_segment(const DCsr& B, Off bs, int len, float a, int32_t* keys, float* vals,
-                                            int32_t* list, int epoch, int& count, bool& bad, int* flags) {
+                                            int epoch, bool& bad, int* flags) {
   const int lane = lane_id();
   for (int q0 = 0; q0 < len; q0 += 32) {
     const int q = q0 + lane;
-    bool fresh = false, failed = false;
-    int32_t j = 0;
+    bool failed = false;
     if (q < len) {
-      j = B.col[bs + q];
+      bool fresh;
+      const int32_t j = B.col[bs + q];
       const float pr = prod_rn(a, B.val[bs + q]);
       const int slot = table_insert(keys, LOGT, j, epoch, fresh);
       if (slot < 0) failed = true;
       else vals[slot] = add_rn(fresh ? 0.f : vals[slot], pr);
     }
-    record_step<LEARNED>(fresh, failed, j, list, count, bad, flags);
+    end_step<LEARNED>(failed, bad, flags);
   }
 }
 
@@ -135,7 +153,7 @@ __device__ __forceinline__ void acc_segment(const DCsr& B, Off bs, int len, floa
 // in canonical order.
 template <int LOGT, bool LEARNED, typename Off>
 __device__ __forceinline__ void acc_packed(const DCsr& B, Off bs, int len, float a, int lo, int hi, int32_t* keys,
-                                           float* vals, int32_t* list, int epoch, int& count, bool& bad, int* flags) {
+                                           float* vals, int epoch, bool& bad, int* flags) {
   const int lane = lane_id();
   const int lr = (lane >= lo && lane < hi) ? len : 0;
   const int incl = warp_incl_scan(lr);
@@ -164,25 +182,24 @@ __device__ __forceinline__ void acc_packed(const DCsr& B, Off bs, int len, float
     float v = (ok && !fresh) ? vals[slot] : 0.f;
     v = group_sum_in_lane_order(grp, pr, v, ok);
     if (ok) vals[slot] = v;
-    record_step<LEARNED>(fresh, leader && slot < 0, j, list, count, bad, flags);
+    end_step<LEARNED>(leader && slot < 0, bad, flags);
   }
 }
 
 // Accumulates row `row` in canonical order (k ascending through A's row,
 // then column ascending through B's row k).  A's row is taken 32 entries at
 // a time: B rows of kPackBelow or more entries go k-serially
-// (acc_segment), runs of shorter ones are packed (acc_packed).  New columns
-// are appended to `list` in the order they are first seen; returns their
-// number, or -1 when LEARNED and the row has more than `cap` distinct
-// columns or filled the table (the learned path's overflow, checked once at
-// the end of the row; the list never exceeds the table).
+// (acc_segment), runs of shorter ones are packed (acc_packed).  At the end
+// the row's columns are gathered from the table into `list`
+// (gather_columns); returns their number, or -1 when LEARNED and the row
+// filled the table or has more than `cap` distinct columns (the learned
+// path's overflow, checked once at the end of the row).
 template <int LOGT, bool R32, bool LEARNED>
 __device__ __forceinline__ int accumulate_row(const DCsr& A, const DCsr& B, int32_t row, int32_t* keys, float* vals,
                                               int32_t* list, int epoch, int cap, int* flags) {
   using Off = typename RowOff<R32>::T;
   const int lane = lane_id();
   const int64_t s = A.rp[row], e = A.rp[row + 1];
-  int count = 0;
   bool bad = false;
   for (int64_t base = s; base < e; base += 32) {
     const int64_t p = base + lane;
@@ -203,18 +220,20 @@ __device__ __forceinline__ int accumulate_row(const DCsr& A, const DCsr& B, int3
         const Off sbs = __shfl_sync(kFull, bs, idx);
         const int sl = __shfl_sync(kFull, len, idx);
         const float sa = __shfl_sync(kFull, a, idx);
-        acc_segment<LOGT, LEARNED>(B, sbs, sl, sa, keys, vals, list, epoch, count, bad, flags);
+        acc_segment<LOGT, LEARNED>(B, sbs, sl, sa, keys, vals, epoch, bad, flags);
         ++idx;
       } else {
         const unsigned later = long_mask & (~0u << idx);
         const int hi = later ? min(n, __ffs(later) - 1) : n;
-        acc_packed<LOGT, LEARNED>(B, bs, len, a, idx, hi, keys, vals, list, epoch, count, bad, flags);
+        acc_packed<LOGT, LEARNED>(B, bs, len, a, idx, hi, keys, vals, epoch, bad, flags);
         idx = hi;
       }
     }
   }
   // the learned capacity is judged once per row: its overflow is rare
-  if (LEARNED && (__any_sync(kFull, bad) || count > cap)) return -1;
+  if (LEARNED && __any_sync(kFull, bad)) return -1;
+  const int count = gather_columns<LOGT>(keys, list, epoch);
+  if (LEARNED && count > cap) return -1;
   return count;
 }
 

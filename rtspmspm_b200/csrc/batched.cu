@@ -127,8 +127,8 @@ __global__ void __launch_bounds__(512, 2) k_batch_bin(const BatchMat* mats, cons
     } else {
       const int64_t base = gscan[M.row_start];
       const int64_t off = M.c_base + (gscan[g] - base);
-      numeric_row<LOGT, true>(M.A, M.B, r, keys, vals, list, ep, c_col + off, c_val + off, gscan[g + 1] - gscan[g],
-                              flags);
+      numeric_row<LOGT, true, true>(M.A, M.B, r, keys, vals, list, ep, c_col + off, c_val + off,
+                                    gscan[g + 1] - gscan[g], flags);
     }
     if (ep >= 0) {
       tagged = true;

@@ -581,7 +581,7 @@ __global__ void __launch_bounds__(512, 2) k_num_warp_learned(DCsr A, DCsr B, con
       }
     } else {
       const int64_t off = slab_off[row];
-      emit_row<LOGT>(keys, vals, list, n, epoch, n, slab_col + off, slab_val + off);
+      emit_row<LOGT>(keys, vals, list, n, epoch, n, slab_col + off, slab_val + off, false);
       if (lane == 0) nnz_out[row] = n;
     }
     next_row<LOGT>(keys, epoch);

@@ -205,10 +205,22 @@ def sample_text(info, what: str) -> str:
     return f"{head} {info['rows']} rows of {what} ({info['products']} products, {info['seconds']:.1f} s)"
 
 
+def workload_config(A, products: int, nnz_c: int, world: int) -> dict:
+    """The `config` object of both arms: the workload and how it is timed."""
+    return {"workload": WORKLOAD, "rows": A.rows, "nnz_a": A.nnz, "products": products, "nnz_c": nnz_c,
+            "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before every step",
+            "index": "int32 CSR"}
+
+
 def reference_arm(args, A):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    from oracle import oracle
+    from rtspmspm_b200 import gen
+
+    products = int(gen.row_products(A, A).sum())
+    nnz_c = int(oracle.row_nnz(A, A).sum())
     per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
     vals = []
     info = None
@@ -223,7 +235,7 @@ def reference_arm(args, A):
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(info["seconds"] / info["passes"] * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": "bounded row sample"},
+        "config": workload_config(A, products, nnz_c, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": round(value, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(value, 4), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -232,90 +244,161 @@ def reference_arm(args, A):
     return 0
 
 
+def timed_median(fn, k, flush, stream):
+    """Median CUDA-event time (ms) of k calls of fn on `stream`, L2 flushed
+    (256 MB write) before each."""
+    import torch
+
+    ts = []
+    for _ in range(k):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def measure_single(eng, A, algos, warmup, steps, flush, stream, index_bits=32):
+    """Per-method timings of C = A*A on device-resident A (validation off):
+    median ms, GFLOP/s, and the stage breakdown, prediction and heavy-row
+    counts of one extra call with stage timing on."""
+    from rtspmspm_b200 import DeviceCsr, _lib, gen
+
+    dA = DeviceCsr.from_host(A, index_bits=index_bits)
+    products = int(gen.row_products(A, A).sum())
+    sa = dA.struct()
+    out = {"rows": A.rows, "nnz_a": A.nnz, "products": products}
+    for algo in algos:
+        o = eng.opts(algo=algo, skip_validation=True, stage_timing=False)
+        for _ in range(warmup):
+            c = _lib.SpgCsr()
+            eng.multiply_raw(sa, sa, o, c, _lib.SpgReport())
+            eng.free_raw(c)
+        holder = {}
+
+        def step():
+            c = _lib.SpgCsr()
+            rep = _lib.SpgReport()
+            eng.multiply_raw(sa, sa, o, c, rep)
+            holder["rep"] = rep
+            eng.free_raw(c)
+
+        ms = timed_median(step, steps, flush, stream)
+        c = _lib.SpgCsr()
+        rep = _lib.SpgReport()
+        eng.multiply_raw(sa, sa, eng.opts(algo=algo, skip_validation=True, stage_timing=True), c, rep)
+        eng.free_raw(c)
+        r = rep.as_dict()
+        out[algo] = {"ms": round(ms, 3), "gflops": round(2 * products / ms / 1e6, 2), "nnz_c": r["nnz_c"],
+                     "stages_ms": {k: round(v, 3) for k, v in r["stages_ms"].items()},
+                     "rows_predicted": r["rows_predicted"], "rows_overflow": r["rows_overflow"],
+                     "rows_heavy": r["rows_heavy"], "kernel_launches": holder["rep"].kernel_launches}
+        if algo == "learned":
+            out[algo]["misprediction_rate"] = round(r["rows_overflow"] / max(1, r["rows_predicted"]), 6)
+    if "plain" in out and "learned" in out:
+        out["speedup_learned_vs_plain"] = round(out["plain"]["ms"] / out["learned"]["ms"], 4)
+    del dA
+    return out
+
+
+CUSPARSE_ALGS = (("ALG1", 1), ("ALG2", 2), ("ALG3", 0))
+
+
+def measure_cusparse(eng, sa, products, warmup, steps, flush, stream):
+    """cuSPARSE SpGEMM on the same GPU, each algorithm (ALG2/ALG3 with chunk
+    fraction 0.01 as the reference's driver) with its own warm-up and median:
+    a reported reference point, not a gate."""
+    from rtspmspm_b200 import _lib
+
+    res = {}
+    for name, code in CUSPARSE_ALGS:
+        o = eng.opts(algo="cusparse", skip_validation=True, cusparse_alg=code)
+        try:
+            for _ in range(warmup):
+                c = _lib.SpgCsr()
+                eng.multiply_raw(sa, sa, o, c, _lib.SpgReport())
+                eng.free_raw(c)
+
+            def step():
+                c = _lib.SpgCsr()
+                eng.multiply_raw(sa, sa, o, c, _lib.SpgReport())
+                eng.free_raw(c)
+
+            ms = timed_median(step, steps, flush, stream)
+            res[name] = {"ms": round(ms, 3), "gflops": round(2 * products / ms / 1e6, 3)}
+        except Exception as ex:  # an algorithm can run out of memory on large products
+            res[name] = {"error": str(ex)[:160]}
+    ok = {k: v for k, v in res.items() if "ms" in v}
+    if ok:
+        res["fastest"] = min(ok, key=lambda k: ok[k]["ms"])
+    res["timing"] = f"median of {steps} after {warmup} warm-up calls, each algorithm"
+    return res
+
+
+def measure_batch(eng, pairs, warmup, steps, flush, stream, tune=True, modes=None):
+    """Batched uneven products: median ms per call of spg_multiply_batched
+    (graph replay and plain stream launches; tuned and default settings)."""
+    from rtspmspm_b200 import DeviceCsr, gen
+
+    dA = [DeviceCsr.from_host(a) for a, _ in pairs]
+    dB = [DeviceCsr.from_host(b) for _, b in pairs]
+    products = sum(int(gen.row_products(a, b).sum()) for a, b in pairs)
+    out = {"products": int(products), "count": len(pairs), "rows": int(sum(a.rows for a, _ in pairs))}
+    if tune:
+        t = time.perf_counter()
+        eng.tune(dA[:min(64, len(dA))], dB[:min(64, len(dB))], None)
+        out["tune_s"] = round(time.perf_counter() - t, 2)
+        out["tuning"] = eng.get_tuning()
+    for graph, tuned in modes or ((True, True), (False, True), (True, False)):
+        if tuned and not tune:
+            continue
+        for _ in range(warmup):
+            eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True)
+        holder = {}
+
+        def step():
+            res, rep = eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True)
+            holder["rep"] = rep
+
+        ms = timed_median(step, steps, flush, stream)
+        key = ("graph" if graph else "stream") + ("_tuned" if tuned else "_default")
+        rep = holder["rep"]
+        out[key] = {"ms": round(ms, 3), "gflops": round(2 * products / ms / 1e6, 2), "nnz_c": rep["nnz_c"],
+                    "kernel_launches": rep["kernel_launches"], "rows_overflow": rep.get("rows_overflow", 0),
+                    "products_individual": rep.get("rows_heavy", 0)}
+    del dA, dB
+    return out
+
+
 def other_workload(args) -> int:
     """Per-method timings for the other configurations (1 GPU):
     rmat20 = C=A*A on R-MAT scale 20 (a=.57, b=c=.19, edge factor 16, seed 0);
     er4096 = C=A*A on the 4,096^2 Erdos-Renyi Poisson(8) matrix (seed 0);
-    batch512 = 512 independent uneven products (seed 1), one persistent
-    launch per stage replayed from a CUDA graph."""
+    batch512 = 512 independent uneven products (seed 1) replayed from a CUDA
+    graph."""
     import torch
 
-    from rtspmspm_b200 import DeviceCsr, Engine, _lib, gen
+    from rtspmspm_b200 import DeviceCsr, Engine, gen
 
     eng = Engine(0, use_torch_stream=True)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     out = {"workload": args.workload, "steps": args.steps, "warmup": args.warmup}
-
-    def timed(fn, k):
-        ts = []
-        for _ in range(k):
-            flush.zero_()
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            fn()
-            e1.record(stream)
-            e1.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        return statistics.median(ts)
-
     if args.workload == "batch512":
-        pairs = gen.batch_uneven(count=args.batch_count, seed=1)
-        dA = [DeviceCsr.from_host(a) for a, _ in pairs]
-        dB = [DeviceCsr.from_host(b) for _, b in pairs]
-        products = sum(int(gen.row_products(a, b).sum()) for a, b in pairs)
-        eng.tune(dA[:min(64, len(dA))], dB[:min(64, len(dB))], None)
-        for graph, tuned in ((True, True), (False, True), (True, False)):
-            for _ in range(args.warmup):
-                eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True)
-            holder = {}
-
-            def step():
-                res, rep = eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True)
-                holder["rep"] = rep
-
-            ms = timed(step, args.steps)
-            key = ("graph" if graph else "stream") + ("_tuned" if tuned else "_default")
-            out[key] = {"ms": round(ms, 3), "gflops": round(2 * products / ms / 1e6, 2),
-                        "nnz_c": holder["rep"]["nnz_c"], "kernel_launches": holder["rep"]["kernel_launches"]}
-        out.update({"products": products, "tuning": eng.get_tuning()})
+        out.update(measure_batch(eng, gen.batch_uneven(count=args.batch_count, seed=1), args.warmup, args.steps,
+                                 flush, stream))
     else:
         A = gen.rmat(args.rmat_scale, 16, seed=0) if args.workload == "rmat20" else gen.erdos_renyi(4096, 4096, 8.0, 0)
-        dA = DeviceCsr.from_host(A)
-        products = int(gen.row_products(A, A).sum())
-        sa = dA.struct()
-        algos = ["plain", "learned"] + (["cusparse"] if args.workload == "er4096" else [])
-        for algo in algos:
-            o = eng.opts(algo=algo, skip_validation=True, stage_timing=False)
-            for _ in range(args.warmup):
-                c = _lib.SpgCsr()
-                eng.multiply_raw(sa, sa, o, c, _lib.SpgReport())
-                eng.free_raw(c)
-            holder = {}
-
-            def step():
-                c = _lib.SpgCsr()
-                rep = _lib.SpgReport()
-                eng.multiply_raw(sa, sa, o, c, rep)
-                holder["rep"] = rep
-                eng.free_raw(c)
-
-            ms = timed(step, args.steps)
-            o2 = eng.opts(algo=algo, skip_validation=True, stage_timing=True)
-            c = _lib.SpgCsr()
-            rep = _lib.SpgReport()
-            eng.multiply_raw(sa, sa, o2, c, rep)
-            eng.free_raw(c)
-            r = rep.as_dict()
-            out[algo] = {"ms": round(ms, 3), "gflops": round(2 * products / ms / 1e6, 2), "nnz_c": r["nnz_c"],
-                         "stages_ms": {k: round(v, 3) for k, v in r["stages_ms"].items()},
-                         "rows_predicted": r["rows_predicted"], "rows_overflow": r["rows_overflow"],
-                         "rows_heavy": r["rows_heavy"]}
-        out.update({"products": products, "rows": A.rows, "nnz_a": A.nnz})
-        if "plain" in out and "learned" in out:
-            out["speedup_learned_vs_plain"] = round(out["plain"]["ms"] / out["learned"]["ms"], 4)
+        out.update(measure_single(eng, A, ["plain", "learned"], args.warmup, args.steps, flush, stream))
+        if args.workload == "er4096":
+            dA = DeviceCsr.from_host(A)
+            out["cusparse"] = measure_cusparse(eng, dA.struct(), out["products"], args.warmup, args.steps, flush,
+                                               stream)
         if args.workload == "rmat20" and not args.no_cpu:
             v, info = cpu_sample(A, args.cpu_seconds)
             out["cpu_baseline"] = {"value": round(v, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
@@ -323,6 +406,26 @@ def other_workload(args) -> int:
     print(json.dumps(out), flush=True)
     eng.close()
     return 0
+
+
+def extra_workloads(args, eng, flush, stream) -> dict:
+    """The other configurations, measured in the same run as the headline so
+    that its line records them (1 GPU only): R-MAT scale 20 and ER 4096
+    (plain vs learned), and the 512 uneven products (graph replay)."""
+    from rtspmspm_b200 import gen
+
+    out = {}
+    t = time.perf_counter()
+    out["er4096"] = measure_single(eng, gen.erdos_renyi(4096, 4096, 8.0, 0), ["plain", "learned"], 3, 20, flush,
+                                   stream)
+    pairs = gen.batch_uneven(count=512, seed=1)
+    out["batch512"] = measure_batch(eng, pairs, 3, max(3, min(args.steps, 10)), flush, stream,
+                                    modes=((True, True), (True, False)))
+    del pairs
+    A = gen.rmat(20, 16, seed=0)
+    out["rmat20"] = measure_single(eng, A, ["plain", "learned"], 1, 3, flush, stream)
+    out["wall_s"] = round(time.perf_counter() - t, 1)
+    return out
 
 
 def main():
@@ -334,6 +437,8 @@ def main():
     ap.add_argument("--grid", type=int, default=96)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the R-MAT-20 / ER-4096 / batch-512 timings that ride on the headline line")
     ap.add_argument("--profile", choices=["plain", "learned"], default=None,
                     help="only W warm-up + K steps of one method (short runs under ncu)")
     ap.add_argument("--workload", choices=["stencil96", "rmat20", "er4096", "batch512"], default="stencil96",
@@ -439,13 +544,9 @@ def main():
     _, rep_ls, _, stages_l, _ = run_steps("learned", 2, stage_timing=True)
     _, rep_ps, _, stages_p, _ = run_steps("plain", 2, stage_timing=True)
 
-    # cuSPARSE SpGEMM (ALG3, as the reference's driver) on the same GPU: reported reference point
-    cus = {}
-    try:
-        ms_c, _, _, _, _ = run_steps("cusparse", 2)
-        cus = {"ms": round(ms_c, 3), "gflops": round(flops / ms_c / 1e6, 3), "alg": "ALG3 chunk 0.01"}
-    except Exception as ex:  # reported, not gated
-        cus = {"error": str(ex)[:200]}
+    # cuSPARSE SpGEMM on the same GPU (ALG1, ALG2 and ALG3, the reference
+    # driver's choice): a reported reference point
+    cus = measure_cusparse(eng, sa, products, 3, 10, flush, stream)
 
     # value-only recompute (structure of C kept, new values): the cuSPARSE
     # reuse flow of the reference's driver
@@ -528,14 +629,17 @@ def main():
             cpu_scipy = {"value": round(sc[0], 4), "unit": "GFLOP/s", "threads": 1,
                          "sample": f"scipy.sparse A[:{sc[1]}] @ A ({sc[2]:.1f} s)"}
 
+    # the other configurations, so that this line records them (1 GPU)
+    extra = None
+    if world == 1 and not args.no_extra:
+        extra = extra_workloads(args, eng, flush, stream)
+
     value = world * flops / (ms_learned * 1e-3) / 1e9
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_learned, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rows": A.rows, "nnz_a": A.nnz, "products": products, "nnz_c": nnz_c,
-                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before every step",
-                   "index": "int32 CSR"},
+        "config": workload_config(A, products, nnz_c, world),
         "plain": {"ms": round(ms_plain, 4), "gflops": round(world * flops / (ms_plain * 1e-3) / 1e9, 3),
                   "stages_ms": {k: round(v, 4) for k, v in stages_p.items()}},
         "learned": {"ms": round(ms_learned, 4), "stages_ms": {k: round(v, 4) for k, v in stages_l.items()},
@@ -553,6 +657,7 @@ def main():
                 "call": f"spg_multiply_into_host, {args.e2e_blocks} row blocks"},
         "gpu_launches": int(round(launches_l * args.steps)),
         "clocks": clocks,
+        "other_workloads": extra,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

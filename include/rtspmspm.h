@@ -217,9 +217,12 @@ spg_status spg_multiply_batched(spg_ctx* ctx, int32_t n, const spg_csr* A, const
  * All scratch lives in one file-scope device array of about 9.3 MB that
  * every GPU loading the library keeps until the process exits; the first
  * call on a device looks up that array's address (make that first call
- * before any stream capture).  Every call shares the array, so calls
- * whose work overlaps on the GPU (other streams, other threads) race and
- * must be serialized by the caller.
+ * before any stream capture).  The address is kept for the life of the
+ * process: do not use this entry point across a cudaDeviceReset.  Every
+ * call shares the array, so calls whose work overlaps on the GPU (other
+ * streams, other threads) race and must be serialized by the caller.  On
+ * an error return the contents of C's buffers are unspecified; a CUDA
+ * error already pending when the call begins is reported, not cleared.
  */
 spg_status spg_multiply_noalloc(void* stream, const spg_csr* A, const spg_csr* B, spg_csr* C,
                                 char* errbuf, int32_t errlen);

@@ -14,7 +14,10 @@
 // at the column count, no more than 2048 with the default tables); larger
 // inputs are rejected with SPG_ERR_UNSUPPORTED/SPG_ERR_INVALID_ARG and a
 // message.  The scratch array (about 9.3 MB) stays resident on every GPU
-// that loads the library until the process exits.
+// that loads the library until the process exits.  Its device address is
+// looked up once per device and kept, so the entry point must not be used
+// across a cudaDeviceReset of that device.  On any error return the
+// contents of C's buffers are unspecified.
 #include <cuda_runtime.h>
 
 #include <cstdarg>
@@ -116,6 +119,12 @@ spg_status check_input(const spg_csr* m, const char* name, char* errbuf, int32_t
 extern "C" spg_status spg_multiply_noalloc(void* stream, const spg_csr* A, const spg_csr* B, spg_csr* C,
                                            char* errbuf, int32_t errlen) {
   if (errbuf && errlen > 0) errbuf[0] = 0;
+  // an error left pending by the caller's earlier work is not this call's:
+  // report it without clearing it, before any device work
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess)
+    return err(errbuf, errlen, SPG_ERR_CUDA, "a CUDA error was already pending when the call began: %s",
+               cudaGetErrorString(pending));
   spg_status st;
   if ((st = check_input(A, "A", errbuf, errlen)) != SPG_OK) return st;
   if ((st = check_input(B, "B", errbuf, errlen)) != SPG_OK) return st;
@@ -184,12 +193,22 @@ extern "C" spg_status spg_multiply_noalloc(void* stream, const spg_csr* A, const
                (long long)big, (long long)bp.warp_cap);
   for (int b = 0; b < kNumWarpBins; ++b)
     launch_sym_warp(kMinLogT + b, dA, dB, lists + off[b], off[b + 1] - off[b], nnz, flags, lc, wpb);
+  NA_CUDA(cudaGetLastError());  // a failed symbolic launch: the counts below would be wrong
   launch_binning(nnz, rows, B->cols, kBinNumeric, bp, bins, counts, offsets, cursors, lists, lc);
   launch_excl_scan(nnz, rows, nnz, scan_tmp, lc);
   int64_t total = 0;
   NA_CUDA(cudaMemcpyAsync(off, offsets, sizeof off, cudaMemcpyDeviceToHost, s));
   NA_CUDA(cudaMemcpyAsync(&total, nnz + rows, sizeof total, cudaMemcpyDeviceToHost, s));
   NA_CUDA(cudaStreamSynchronize(s));
+  // only the warp bins are launched below: a non-empty row binned anywhere
+  // else would leave its part of C unwritten
+  int64_t outside = 0;
+  for (int b = kNumWarpBins; b < kNumBins; ++b)
+    if (b != kBinEmpty) outside += off[b + 1] - off[b];
+  if (outside > 0)
+    return err(errbuf, errlen, SPG_ERR_INTERNAL,
+               "%lld output rows exceed the warp hash tables after the exact count (internal binning mismatch)",
+               (long long)outside);
   C->rows = rows;
   C->cols = B->cols;
   if (total > C->capacity) {
@@ -203,6 +222,7 @@ extern "C" spg_status spg_multiply_noalloc(void* stream, const spg_csr* A, const
   for (int b = 0; b < kNumWarpBins; ++b)
     launch_num_warp(kMinLogT + b, dA, dB, lists + off[b], off[b + 1] - off[b], nnz, C->col_idx, C->val, flags, lc,
                     wpb);
+  NA_CUDA(cudaGetLastError());
   if (C->index_bits == 64)
     NA_CUDA(cudaMemcpyAsync(C->row_ptr, nnz, (size_t)(rows + 1) * 8, cudaMemcpyDeviceToDevice, s));
   else

@@ -72,6 +72,46 @@ def test_batch_with_a_heavy_product_falls_back_per_product():
         eng.close()
 
 
+def _digest(H):
+    """Order-sensitive digest of a host CSR (row pointers, columns, value bits)."""
+    rp = np.asarray(H.row_ptr, np.int64)
+    col = np.asarray(H.col_idx, np.int64)
+    bits = np.asarray(H.val, np.float32).view(np.uint32).astype(np.uint64)
+    w = np.arange(1, col.size + 1, dtype=np.uint64)
+    return (int(rp.sum()), int(col.sum()), int((col.astype(np.uint64) * w).sum()), int(bits.sum()),
+            int((bits * w).sum()))
+
+
+def test_batch512_full_size_capture_then_replay():
+    """The 512 uneven products (seed 1; rows, inner and column dimensions
+    log-uniform on [1k, 64k], Poisson nnz/row with means U(2, 32)) through one
+    batched call captured as a CUDA graph, then replayed: every product of
+    the replay is checked whole against the oracle, and the captured call's
+    output is bit-identical to the replay's."""
+    pairs = gen.batch_uneven(count=512, seed=1)
+    eng = Engine(0)
+    try:
+        dA = [DeviceCsr.from_host(a) for a, _ in pairs]
+        dB = [DeviceCsr.from_host(b) for _, b in pairs]
+        res, rep = eng.multiply_batched(dA, dB, use_graph=True)
+        assert rep["device_flags"] == 0
+        first = [_digest(C.to_host()) for C in res]
+        res, rep = eng.multiply_batched(dA, dB, use_graph=True)
+        assert rep["device_flags"] == 0
+        assert rep["products"] == sum(int(gen.row_products(a, b).sum()) for a, b in pairs)
+        tot = 0
+        for i, ((A, B), C) in enumerate(zip(pairs, res)):
+            H = C.to_host()
+            assert _digest(H) == first[i], f"product {i}: replay differs from the captured call"
+            R = oracle.spgemm(A, B)
+            assert_parity(H, R)
+            tot += R.nnz
+            del H, R
+        assert rep["nnz_c"] == tot
+    finally:
+        eng.close()
+
+
 def test_autotuner_cache(tmp_path):
     A = gen.stencil27(20)
     eng = Engine(0)

@@ -13,7 +13,9 @@ from rtspmspm_b200.gen import coo_to_csr
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF_UTIL = os.path.join(ROOT, "oracle", "_ref", "libref_util.so")
-REF_DATA = "/root/reference/optixSpMSpM/src/data"
+from oracle import reference_root
+
+REF_DATA = os.path.join(reference_root() or "", "optixSpMSpM", "src", "data")
 
 
 def ref_util():

@@ -229,6 +229,8 @@ namespace {
 
 // Largest blocked index of B built for the heavy-row tiles (bytes).
 constexpr size_t kBlockedIndexMaxBytes = size_t(4) << 30;
+// Largest list of non-empty heavy-row tiles (bytes).
+constexpr size_t kWorkListMaxBytes = size_t(4) << 30;
 
 // Buffers and host mirrors of one multiply call.
 struct Pipeline {
@@ -337,8 +339,24 @@ struct Pipeline {
     }
     const int64_t nheavy = bin_size(kBinHeavy);
     if (nheavy > 0) {
+      size_t free_b = 0, total_b = 0;
+      cudaMemGetInfo(&free_b, &total_b);
+      // the list of non-empty (row, tile) units for the tile kernel, when it
+      // fits: rows of wide products touch a small part of their tiles
+      const size_t work_bytes = (size_t)nheavy * (size_t)ntiles * 8;
+      const bool use_list = tune.heavy_path != 1 && ntiles > 1 && work_bytes <= kWorkListMaxBytes &&
+                            work_bytes < free_b / 4;
+      DevBuf nz, work;
+      if (use_list) SPG_TRY(nz.alloc(ctx, (size_t)(nheavy + 1) * 8));
       launch_tile_offsets(bin_rows(kBinHeavy), nheavy, big_slot.as<int32_t>(), tile_cnt.as<int32_t>(), ntiles,
-                          tile_off.as<int32_t>(), lc);
+                          tile_off.as<int32_t>(), use_list ? nz.as<int64_t>() : nullptr, lc);
+      if (use_list) {
+        SPG_TRY(work.alloc(ctx, work_bytes));
+        launch_excl_scan(nz.as<int64_t>(), nheavy, nz.as<int64_t>(), scan_tmp.as<int64_t>(), lc);
+        launch_tile_worklist(bin_rows(kBinHeavy), nheavy, big_slot.as<int32_t>(), tile_cnt.as<int32_t>(), ntiles,
+                             nz.as<int64_t>(), work.as<int64_t>(), lc);
+        ctx->launches += 5;
+      }
       // staged path (opt-in): each heavy row's products walked once into
       // per-tile buckets; measured slower than rescanning on R-MAT (the
       // bucket writes scatter over a buffer far larger than L2)
@@ -351,8 +369,6 @@ struct Pipeline {
         // budget (else per-tile binary searches)
         DevBuf bidx;
         const size_t bidx_bytes = (size_t)B.view.rows * (size_t)(ntiles + 1) * 4;
-        size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
         const bool use_index = ntiles > 1 && bidx_bytes <= kBlockedIndexMaxBytes && bidx_bytes < free_b / 4;
         DevBuf tocc;
         if (use_index) {
@@ -365,6 +381,7 @@ struct Pipeline {
         launch_num_tile(A.view, B.view, bin_rows(kBinHeavy), nheavy, big_slot.as<int32_t>(),
                         tile_cnt.as<int32_t>(), tile_off.as<int32_t>(), ntiles, c_rp, c_col, c_val,
                         use_index ? bidx.as<int32_t>() : nullptr, use_index ? tocc.as<uint32_t>() : nullptr,
+                        use_list ? work.as<int64_t>() : nullptr, use_list ? nz.as<int64_t>() + nheavy : nullptr,
                         ctx->d_counter, ctx->d_flags, lc);
         ctx->launches += 2;
       }

@@ -115,6 +115,19 @@ __device__ __forceinline__ int warp_upper_bound(int incl, int t) {
   return lo;
 }
 
+// First lane l whose (nondecreasing) value v[l] exceeds t, for any integer
+// type; requires t < v[31].
+template <typename T>
+__device__ __forceinline__ int warp_upper_bound_t(T v, T t) {
+  int lo = 0;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    const T x = __shfl_sync(kFull, v, lo + s - 1);
+    if (x <= t) lo += s;
+  }
+  return lo;
+}
+
 // Product in the reference's arithmetic: rounded to FP32, no contraction.
 __device__ __forceinline__ float prod_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }

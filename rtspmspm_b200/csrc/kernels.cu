@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "kernels.hpp"
+#include "block_row.cuh"
 #include "tile.cuh"
 #include "warp_row.cuh"
 
@@ -299,19 +300,6 @@ __global__ void __launch_bounds__(512, 2) k_sym_warp(DCsr A, DCsr B, const int32
     if (lane == 0) nnz_out[row] = cnt;
     if (epoch >= 0) next_row<LOGT>(keys, epoch);
   }
-}
-
-// First lane l whose (nondecreasing) value v[l] exceeds t, for any integer
-// type; requires t < v[31].
-template <typename T>
-__device__ __forceinline__ int warp_upper_bound_t(T v, T t) {
-  int lo = 0;
-#pragma unroll
-  for (int s = 16; s > 0; s >>= 1) {
-    const T x = __shfl_sync(kFull, v, lo + s - 1);
-    if (x <= t) lo += s;
-  }
-  return lo;
 }
 
 // Visits every product column of `row` with the whole CTA (NTHR threads), in
@@ -700,21 +688,44 @@ __global__ void k_tile_counts_from_cols(const int32_t* heavy_rows, int64_t nheav
   }
 }
 
-// Per heavy row: exclusive scan of its tile counts (warp per row slot).
+// Per heavy row: exclusive scan of its tile counts (warp per row slot) and,
+// when nz_cnt is given, the number of its tiles with output entries.
 __global__ void k_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
-                               const int32_t* tile_cnt, int ntiles, int32_t* tile_off) {
+                               const int32_t* tile_cnt, int ntiles, int32_t* tile_off, int64_t* nz_cnt) {
   const int lane = lane_id();
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t h = gw; h < nheavy; h += nw) {
     const int64_t slot = big_slot[heavy_rows[h]];
-    int carry = 0;
+    int carry = 0, nz = 0;
     for (int t0 = 0; t0 < ntiles; t0 += 32) {
       const int t = t0 + lane;
       const int v = t < ntiles ? tile_cnt[slot * ntiles + t] : 0;
       const int inc = warp_incl_scan(v);
       if (t < ntiles) tile_off[slot * ntiles + t] = carry + inc - v;
       carry += __shfl_sync(kFull, inc, 31);
+      nz += __popc(__ballot_sync(kFull, v > 0));
+    }
+    if (nz_cnt && lane == 0) nz_cnt[h] = nz;
+  }
+}
+
+// The (heavy row, tile) units with output entries, as h * ntiles + tile,
+// row after row from the exclusive scan nz_off of the per-row counts.
+__global__ void k_tile_worklist(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
+                                const int32_t* tile_cnt, int ntiles, const int64_t* nz_off, int64_t* work) {
+  const int lane = lane_id();
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t h = gw; h < nheavy; h += nw) {
+    const int64_t slot = big_slot[heavy_rows[h]];
+    int64_t pos = nz_off[h];
+    for (int t0 = 0; t0 < ntiles; t0 += 32) {
+      const int t = t0 + lane;
+      const bool nz = t < ntiles && tile_cnt[slot * ntiles + t] > 0;
+      const unsigned m = __ballot_sync(kFull, nz);
+      if (nz) work[pos + __popc(m & ((1u << lane) - 1u))] = h * (int64_t)ntiles + t;
+      pos += __popc(m);
     }
   }
 }
@@ -837,8 +848,11 @@ __device__ __forceinline__ void tile_packed(const DCsr& B, Off bs, int len, floa
   }
 }
 
-// One warp per (heavy row, 2^kTileShift-column tile), tiles handed out by an atomic
-// ticket.  A's row is read 32 entries at a time (the next 32 loaded while the
+// Units of the tile kernel handed out per atomic ticket.
+constexpr int kTicketTiles = 4;
+
+// One warp per (heavy row, 2^kTileShift-column tile), kTicketTiles tiles
+// handed out per atomic ticket (from the list of non-empty tiles when given).  A's row is read 32 entries at a time (the next 32 loaded while the
 // current ones are processed); each entry's B row is narrowed to the tile
 // (blocked index, else binary search) and the segments are accumulated in
 // canonical order (k ascending, then column): long segments by the whole
@@ -850,8 +864,9 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
                                                         const int32_t* big_slot, const int32_t* tile_cnt,
                                                         const int32_t* tile_off, int ntiles, const int64_t* c_rp,
                                                         int32_t* c_col, float* c_val, const int32_t* bidx,
-                                                        const uint32_t* tocc, int twords,
-                                                        unsigned long long* tile_counter, int* flags) {
+                                                        const uint32_t* tocc, int twords, const int64_t* work,
+                                                        const int64_t* nwork, unsigned long long* tile_counter,
+                                                        int* flags) {
   using Off = typename RowOff<R32>::T;
   extern __shared__ uint32_t sm_tile[];
   const int lane = lane_id(), wib = threadIdx.x >> 5;
@@ -861,14 +876,20 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
   for (int s = lane; s < kTileCols; s += 32) acc[s] = 0.f;
   for (int s = lane; s < kTileWords; s += 32) bits[s] = 0u;
   __syncwarp();
-  const int64_t total_tiles = nheavy * (int64_t)ntiles;
-  for (;;) {
-    unsigned long long t = 0;
-    if (lane == 0) t = atomicAdd(tile_counter, 1ull);
-    t = __shfl_sync(kFull, t, 0);
-    if ((int64_t)t >= total_tiles) break;
-    const int64_t h = (int64_t)t / ntiles;
-    const int tile = (int)((int64_t)t % ntiles);
+  // units: the listed non-empty tiles, else every (row, tile)
+  const int64_t units = work ? *nwork : nheavy * (int64_t)ntiles;
+  for (int64_t u = kTicketTiles, u_end = 0;; ++u) {
+    if (u >= u_end) {
+      // the next kTicketTiles units for one atomic
+      unsigned long long t = 0;
+      if (lane == 0) t = atomicAdd(tile_counter, 1ull);
+      u = (int64_t)__shfl_sync(kFull, t, 0) * kTicketTiles;
+      if (u >= units) break;
+      u_end = min(units, u + kTicketTiles);
+    }
+    const int64_t id = work ? work[u] : u;
+    const int64_t h = id / ntiles;
+    const int tile = (int)(id % ntiles);
     const int32_t row = heavy_rows[h];
     const int64_t slot = big_slot[row];
     const int want = tile_cnt[slot * ntiles + tile];
@@ -1299,10 +1320,17 @@ void launch_tile_counts_from_cols(const int32_t* heavy_rows, int64_t nheavy, con
 }
 
 void launch_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot, const int32_t* tile_cnt,
-                         int ntiles, int32_t* tile_off, const LaunchCtx& lc) {
+                         int ntiles, int32_t* tile_off, int64_t* nz_cnt, const LaunchCtx& lc) {
   if (nheavy == 0) return;
   k_tile_offsets<<<grid_for(nheavy, 256, 32, lc.sms * 8), 256, 0, lc.stream>>>(heavy_rows, nheavy, big_slot, tile_cnt,
-                                                                                ntiles, tile_off);
+                                                                                ntiles, tile_off, nz_cnt);
+}
+
+void launch_tile_worklist(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot, const int32_t* tile_cnt,
+                          int ntiles, const int64_t* nz_off, int64_t* work, const LaunchCtx& lc) {
+  if (nheavy == 0) return;
+  k_tile_worklist<<<grid_for(nheavy, 256, 32, lc.sms * 8), 256, 0, lc.stream>>>(heavy_rows, nheavy, big_slot,
+                                                                                 tile_cnt, ntiles, nz_off, work);
 }
 
 void launch_build_blocked_index(const DCsr& B, int ntiles, int32_t* bidx, const LaunchCtx& lc) {
@@ -1314,7 +1342,8 @@ template <bool R32>
 static void num_tile_one(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy,
                          const int32_t* big_slot, const int32_t* tile_cnt, const int32_t* tile_off, int ntiles,
                          const int64_t* c_rp, int32_t* c_col, float* c_val, const int32_t* bidx,
-                         const uint32_t* tocc, unsigned long long* tile_counter, int* flags, const LaunchCtx& lc) {
+                         const uint32_t* tocc, const int64_t* work, const int64_t* nwork,
+                         unsigned long long* tile_counter, int* flags, const LaunchCtx& lc) {
   const size_t smem = (size_t)kTileWarps * (kTileCols + kTileWords + 32) * 4;
   const int twords = (ntiles + 31) / 32;
   cudaFuncSetAttribute(k_num_tile<R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1326,20 +1355,20 @@ static void num_tile_one(const DCsr& A, const DCsr& B, const int32_t* heavy_rows
   cudaMemsetAsync(tile_counter, 0, sizeof(unsigned long long), lc.stream);
   k_num_tile<R32><<<blocks, kTileWarps * 32, smem, lc.stream>>>(A, B, heavy_rows, nheavy, big_slot, tile_cnt,
                                                                 tile_off, ntiles, c_rp, c_col, c_val, bidx, tocc,
-                                                                twords, tile_counter, flags);
+                                                                twords, work, nwork, tile_counter, flags);
 }
 
 void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
                      const int32_t* tile_cnt, const int32_t* tile_off, int ntiles, const int64_t* c_rp,
-                     int32_t* c_col, float* c_val, const int32_t* bidx, const uint32_t* tocc,
-                     unsigned long long* tile_counter, int* flags, const LaunchCtx& lc) {
+                     int32_t* c_col, float* c_val, const int32_t* bidx, const uint32_t* tocc, const int64_t* work,
+                     const int64_t* nwork, unsigned long long* tile_counter, int* flags, const LaunchCtx& lc) {
   if (nheavy == 0) return;
   if (B.rp32)
     num_tile_one<true>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off, ntiles, c_rp, c_col, c_val, bidx,
-                       tocc, tile_counter, flags, lc);
+                       tocc, work, nwork, tile_counter, flags, lc);
   else
     num_tile_one<false>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off, ntiles, c_rp, c_col, c_val, bidx,
-                        tocc, tile_counter, flags, lc);
+                        tocc, work, nwork, tile_counter, flags, lc);
 }
 
 void launch_build_tile_occupancy(int64_t rows, const int32_t* bidx, int ntiles, uint32_t* tocc, const LaunchCtx& lc) {

@@ -82,17 +82,24 @@ void launch_row_lengths(const int64_t* rp, int64_t rows, int64_t* len, const Lau
 void launch_tile_counts_from_cols(const int32_t* heavy_rows, int64_t nheavy, const int64_t* c_rp,
                                   const int32_t* c_col, int ntiles, int32_t* big_slot, int32_t* tile_cnt, int* flags,
                                   const LaunchCtx& lc);
+// Per heavy row: tile offsets (scan of the tile counts) and, when nz_cnt is
+// given, its number of non-empty tiles.
 void launch_tile_offsets(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot, const int32_t* tile_cnt,
-                         int ntiles, int32_t* tile_off, const LaunchCtx& lc);
+                         int ntiles, int32_t* tile_off, int64_t* nz_cnt, const LaunchCtx& lc);
+// The non-empty (heavy row, tile) units, h * ntiles + tile, at nz_off[h].
+void launch_tile_worklist(const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot, const int32_t* tile_cnt,
+                          int ntiles, const int64_t* nz_off, int64_t* work, const LaunchCtx& lc);
 void launch_build_blocked_index(const DCsr& B, int ntiles, int32_t* bidx, const LaunchCtx& lc);
 // Tile occupancy bits of B from its blocked index (ceil(ntiles / 32) words per row).
 void launch_build_tile_occupancy(int64_t rows, const int32_t* bidx, int ntiles, uint32_t* tocc, const LaunchCtx& lc);
 // bidx: blocked index of B (launch_build_blocked_index) or null (binary
-// searches); tocc: its occupancy bits or null
+// searches); tocc: its occupancy bits or null; work/nwork: the list of
+// non-empty tiles (launch_tile_worklist) and its length on the device, or
+// null (every tile is visited)
 void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
                      const int32_t* tile_cnt, const int32_t* tile_off, int ntiles, const int64_t* c_rp,
-                     int32_t* c_col, float* c_val, const int32_t* bidx, const uint32_t* tocc,
-                     unsigned long long* tile_counter, int* flags, const LaunchCtx& lc);
+                     int32_t* c_col, float* c_val, const int32_t* bidx, const uint32_t* tocc, const int64_t* work,
+                     const int64_t* nwork, unsigned long long* tile_counter, int* flags, const LaunchCtx& lc);
 void launch_compact_rows(const int32_t* rows, int64_t nrows, const uint8_t* need_exact, const int64_t* slab_off,
                          const int32_t* slab_col, const float* slab_val, const int64_t* c_rp, int32_t* c_col,
                          float* c_val, const LaunchCtx& lc);

@@ -351,7 +351,10 @@ typedef struct spg_tuning {
     int32_t heavy_path;        /* rows beyond the warp tables: 0 = every column tile rescans
                                   its row of A; 1 = products staged once per tile in HBM
                                   buckets when they fit (else as 0) */
-    int32_t reserved[3];
+    int32_t block_min_nnz;     /* rows with more output entries than this (and at most 8192)
+                                  use a CTA-wide hash table; 0: those beyond a 2^10-slot
+                                  warp table at max_load; -1: off (warp tables and tiles) */
+    int32_t reserved[2];
 } spg_tuning;
 
 spg_status spg_get_tuning(spg_ctx* ctx, spg_tuning* out);

@@ -91,6 +91,13 @@ BinParams bin_params(const spg_tuning& t) {
   // symbolic CTA table at load <= 2/3
   int blg = ilog2_floor(std::max(1024, std::min(32768, t.block_table_max)));
   bp.block_cap = ((int64_t)1 << blg) * 2 / 3;
+  // CTA-wide numeric hash bins (tables at load <= 1/2: their key and
+  // order-word arrays are the row sort's buffers) for rows above the warp
+  // tables that stay efficient: by default those of more than 2^10 slots
+  if (t.block_min_nnz < 0) return without_block_bins(bp);
+  bp.block_min = t.block_min_nnz > 0 ? (int64_t)t.block_min_nnz : (int64_t)std::floor(1024.0 * bp.max_load);
+  bp.blk_small_cap = ((int64_t)1 << kBlkLogSmallT) / 2;
+  bp.blk_large_cap = ((int64_t)1 << kBlkLogLargeT) / 2;
   return bp;
 }
 
@@ -337,6 +344,12 @@ struct Pipeline {
                       wpb);
       ++ctx->launches;
     }
+    // rows above the efficient warp tables: CTA-wide hash tables
+    for (int b : {kBinBlock, kBinDense}) {
+      if (bin_size(b) == 0) continue;
+      launch_num_block(b, A.view, B.view, bin_rows(b), bin_size(b), c_rp, c_col, c_val, ctx->d_flags, lc);
+      ++ctx->launches;
+    }
     const int64_t nheavy = bin_size(kBinHeavy);
     if (nheavy > 0) {
       size_t free_b = 0, total_b = 0;
@@ -491,9 +504,12 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
   tm.mark(SPG_STAGE_MLP);
   // d_counter: [1] products, [2] overflowed rows, [3] rows predicted heavy
   SPG_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, 4 * 8, ctx->stream));
-  launch_learned_plan(P.A.view, P.B.view, ctx->mlp_w16, P.tune.predict_margin, P.tune.predict_slack, P.bp.warp_cap,
-                      o.force_overflow, P.prod.as<int64_t>(), cap.as<int64_t>(), need.as<uint8_t>(),
-                      ctx->d_counter + 3, lc);
+  // rows up to the largest CTA table are sized by the prediction (with the
+  // CTA bins off, up to the largest warp table and as the predicted bin says)
+  const bool cta_bins = P.bp.blk_large_cap > 0;
+  launch_learned_plan(P.A.view, P.B.view, ctx->mlp_w16, P.tune.predict_margin, P.tune.predict_slack,
+                      std::max(P.bp.warp_cap, P.bp.blk_large_cap), cta_bins ? 0 : 1, o.force_overflow,
+                      P.prod.as<int64_t>(), cap.as<int64_t>(), need.as<uint8_t>(), ctx->d_counter + 3, lc);
   launch_sum(P.prod.as<int64_t>(), rows, ctx->d_counter + 1, lc);
   ctx->launches += 2;
   tm.mark(SPG_STAGE_BINNING);
@@ -511,8 +527,10 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
   SPG_TRY(stage_read(ctx, ctx->h_stage + kExactSlot, ctx->d_counter + 3, 8));
   SPG_TRY(P.fetch_offsets(slab_off.as<int64_t>() + rows, &slab_total, 1));
   const int64_t n_exact = ctx->h_stage[kExactSlot];
+  // predicted-light rows: the warp bins and the CTA bins, the first
+  // entries of the binning's lists
   int64_t light = 0;
-  for (int b = 0; b < kNumWarpBins; ++b) light += P.bin_size(b);
+  for (int b = 0; b <= kBinDense; ++b) light += P.bin_size(b);
   if (rep) rep->rows_predicted = light;
   // single numeric pass for the predicted-light rows
   DevBuf slab_col, slab_val, retry;
@@ -525,6 +543,13 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
     launch_num_warp_learned(kMinLogT + b, P.A.view, P.B.view, P.bin_rows(b), P.bin_size(b), cap.as<int64_t>(),
                             slab_off.as<int64_t>(), slab_col.as<int32_t>(), slab_val.as<float>(), P.nnz.as<int64_t>(),
                             retry.as<int32_t>(), ctx->d_counter + 2, ctx->d_flags, lc, P.wpb);
+    ++ctx->launches;
+  }
+  for (int b : {kBinBlock, kBinDense}) {
+    if (P.bin_size(b) == 0) continue;
+    launch_num_block_learned(b, P.A.view, P.B.view, P.bin_rows(b), P.bin_size(b), cap.as<int64_t>(),
+                             slab_off.as<int64_t>(), slab_col.as<int32_t>(), slab_val.as<float>(), P.nnz.as<int64_t>(),
+                             retry.as<int32_t>(), ctx->d_counter + 2, ctx->d_flags, lc);
     ++ctx->launches;
   }
   // exact path for predicted-heavy rows plus overflowed rows; with neither

@@ -233,7 +233,7 @@ std::vector<uintptr_t> plan_key(spg_ctx* ctx, int n, const spg_csr* A, const spg
 // Issues the device work of one batched execution on ctx->stream.
 void enqueue(spg_ctx* ctx, BatchPlan* p) {
   const LaunchCtx lc = launch_ctx(ctx);
-  const BinParams bp = bin_params(p->tune);
+  const BinParams bp = without_block_bins(bin_params(p->tune));
   int launches = 0;
   const int64_t R = p->R;
   auto blocks_for = [&](int64_t work, int per_block) {
@@ -303,7 +303,7 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
   // every warp table size stays available on the batched path: a smaller
   // tuned maximum would send whole products to the one-by-one path
   p->tune.warp_table_max = default_tuning().warp_table_max;
-  const BinParams bp = bin_params(p->tune);
+  const BinParams bp = without_block_bins(bin_params(p->tune));
   const LaunchCtx lc = launch_ctx(ctx);
   p->mats.resize((size_t)n);
   int64_t R = 0;

@@ -29,10 +29,6 @@ namespace spg {
 
 constexpr int kBlkThreads = 256;
 constexpr int kBlkWarps = kBlkThreads / 32;
-// Log2 of the CTA tables of the two CTA bins (numeric/learned binning).
-constexpr int kBlkLogSmall = 12;
-constexpr int kBlkLogLarge = 14;
-
 // Shared scratch of the CTA accumulator besides its table: the staged chunk
 // of A's row while accumulating, the radix histograms while sorting.
 struct BlockScratch {

@@ -116,7 +116,13 @@ __device__ __forceinline__ int bin_of(int64_t key, int64_t cols, int mode, const
     return kBinDense;
   }
   if (key <= 0) return kBinEmpty;
-  if (key <= bp.warp_cap) {
+  const bool warp_ok = key <= bp.warp_cap;
+  if (!(warp_ok && key <= bp.block_min)) {
+    // the CTA-wide hash bins
+    if (key <= bp.blk_small_cap) return kBinBlock;
+    if (key <= bp.blk_large_cap) return kBinDense;
+  }
+  if (warp_ok) {
     int64_t need = (int64_t)ceilf((float)key / bp.max_load);
     int lg = ceil_log2_i64(need);
     if (lg < kMinLogT) lg = kMinLogT;
@@ -573,6 +579,65 @@ __global__ void __launch_bounds__(512, 2) k_num_warp_learned(DCsr A, DCsr B, con
       if (lane == 0) nnz_out[row] = n;
     }
     next_row<LOGT>(keys, epoch);
+  }
+}
+
+// --------------------------------------------------------------------------
+// Numeric pass: CTA-wide hash accumulator (block_row.cuh)
+// --------------------------------------------------------------------------
+
+// Plain numeric pass, one CTA per row of the bin: exact nnz known, written
+// straight into C.
+template <int LOGT, bool R32>
+__global__ void __launch_bounds__(kBlkThreads) k_num_block(DCsr A, DCsr B, const int32_t* rows, int64_t nrows,
+                                                           const int64_t* c_rp, int32_t* c_col, float* c_val,
+                                                           int* flags) {
+  constexpr int T = 1 << LOGT;
+  extern __shared__ int32_t sm_blk[];
+  __shared__ BlockScratch sc;
+  int32_t* keys = sm_blk;
+  float* vals = reinterpret_cast<float*>(sm_blk + T);
+  uint32_t* own = reinterpret_cast<uint32_t*>(sm_blk + 2 * T);
+  for (int64_t idx = blockIdx.x; idx < nrows; idx += gridDim.x) {
+    const int32_t row = rows[idx];
+    const int64_t off = c_rp[row];
+    const int64_t want = c_rp[row + 1] - off;
+    const int n = cta_accumulate_row<LOGT, R32, false>(A, B, row, keys, vals, own, sc, 0, flags);
+    if (n != want && threadIdx.x == 0) raise_flag(flags, kFlagCountDiff);
+    cta_emit_row<LOGT>(keys, vals, own, sc, n, want, c_col + off, c_val + off);
+  }
+}
+
+// Learned single pass, one CTA per row: the row is written sorted into its
+// slab slot; a row with more distinct columns than its capacity is queued
+// for the exact re-run (nnz_out = -1).
+template <int LOGT, bool R32>
+__global__ void __launch_bounds__(kBlkThreads) k_num_block_learned(DCsr A, DCsr B, const int32_t* rows,
+                                                                   int64_t nrows, const int64_t* cap,
+                                                                   const int64_t* slab_off, int32_t* slab_col,
+                                                                   float* slab_val, int64_t* nnz_out,
+                                                                   int32_t* retry_rows,
+                                                                   unsigned long long* retry_count, int* flags) {
+  constexpr int T = 1 << LOGT;
+  extern __shared__ int32_t sm_blk[];
+  __shared__ BlockScratch sc;
+  int32_t* keys = sm_blk;
+  float* vals = reinterpret_cast<float*>(sm_blk + T);
+  uint32_t* own = reinterpret_cast<uint32_t*>(sm_blk + 2 * T);
+  for (int64_t idx = blockIdx.x; idx < nrows; idx += gridDim.x) {
+    const int32_t row = rows[idx];
+    const int n = cta_accumulate_row<LOGT, R32, true>(A, B, row, keys, vals, own, sc, cap[row], flags);
+    if (n < 0) {
+      if (threadIdx.x == 0) {
+        nnz_out[row] = -1;
+        const unsigned long long pos = atomicAdd(retry_count, 1ull);
+        retry_rows[pos] = row;
+      }
+      continue;
+    }
+    const int64_t off = slab_off[row];
+    cta_emit_row<LOGT>(keys, vals, own, sc, n, n, slab_col + off, slab_val + off);
+    if (threadIdx.x == 0) nnz_out[row] = n;
   }
 }
 
@@ -1279,6 +1344,66 @@ void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int3
     default: break;
   }
 #undef SPG_NWL
+}
+
+template <int LOGT, bool R32>
+static int block_grid(const void* kernel, int64_t nrows, const LaunchCtx& lc) {
+  const size_t smem = (size_t)block_words<LOGT>() * 4;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlkThreads, smem);
+  if (per_sm < 1) per_sm = 1;
+  return (int)std::min<int64_t>(nrows, (int64_t)lc.sms * per_sm);
+}
+
+template <int LOGT, bool R32>
+static void num_block_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, const int64_t* c_rp,
+                          int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc) {
+  const size_t smem = (size_t)block_words<LOGT>() * 4;
+  const int blocks = block_grid<LOGT, R32>((const void*)k_num_block<LOGT, R32>, nrows, lc);
+  k_num_block<LOGT, R32><<<blocks, kBlkThreads, smem, lc.stream>>>(A, B, rows, nrows, c_rp, c_col, c_val, flags);
+}
+
+template <int LOGT, bool R32>
+static void num_block_learned_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
+                                  const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
+                                  int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
+                                  const LaunchCtx& lc) {
+  const size_t smem = (size_t)block_words<LOGT>() * 4;
+  const int blocks = block_grid<LOGT, R32>((const void*)k_num_block_learned<LOGT, R32>, nrows, lc);
+  k_num_block_learned<LOGT, R32><<<blocks, kBlkThreads, smem, lc.stream>>>(A, B, rows, nrows, cap, slab_off,
+                                                                           slab_col, slab_val, nnz_out, retry_rows,
+                                                                           retry_count, flags);
+}
+
+void launch_num_block(int bin, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, const int64_t* c_rp,
+                      int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc) {
+  if (nrows == 0) return;
+  if (bin == kBinBlock) {
+    if (B.rp32) num_block_one<kBlkLogSmallT, true>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc);
+    else num_block_one<kBlkLogSmallT, false>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc);
+  } else {
+    if (B.rp32) num_block_one<kBlkLogLargeT, true>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc);
+    else num_block_one<kBlkLogLargeT, false>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc);
+  }
+}
+
+void launch_num_block_learned(int bin, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
+                              const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
+                              int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
+                              const LaunchCtx& lc) {
+  if (nrows == 0) return;
+#define SPG_NBL(L, R)                                                                                            \
+  num_block_learned_one<L, R>(A, B, rows, nrows, cap, slab_off, slab_col, slab_val, nnz_out, retry_rows,       \
+                              retry_count, flags, lc)
+  if (bin == kBinBlock) {
+    if (B.rp32) SPG_NBL(kBlkLogSmallT, true);
+    else SPG_NBL(kBlkLogSmallT, false);
+  } else {
+    if (B.rp32) SPG_NBL(kBlkLogLargeT, true);
+    else SPG_NBL(kBlkLogLargeT, false);
+  }
+#undef SPG_NBL
 }
 
 // dst[i] = src[i] for n 32-bit words; dst may be mapped pinned host memory.

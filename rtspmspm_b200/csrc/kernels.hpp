@@ -17,11 +17,15 @@ struct DCsr;
 constexpr int kMinLogT = 5;
 constexpr int kMaxLogT = 12;
 constexpr int kNumWarpBins = kMaxLogT - kMinLogT + 1;  // 8
-constexpr int kBinBlock = 8;   // symbolic: CTA hash table
-constexpr int kBinDense = 9;   // symbolic: CTA bitmap over the column span
+constexpr int kBinBlock = 8;   // symbolic: CTA hash table; numeric: CTA hash of 2^12 slots
+constexpr int kBinDense = 9;   // symbolic: CTA bitmap over the column span; numeric: CTA hash of 2^14 slots
 constexpr int kBinHeavy = 10;  // numeric: column-tiled heavy rows
 constexpr int kBinEmpty = 11;  // no products
 constexpr int kNumBins = 12;
+
+// Log2 of the CTA-wide numeric hash tables of kBinBlock / kBinDense.
+constexpr int kBlkLogSmallT = 12;
+constexpr int kBlkLogLargeT = 14;
 
 constexpr int kBinSymbolic = 0;
 constexpr int kBinNumeric = 1;
@@ -39,7 +43,22 @@ struct BinParams {
   int64_t block_cap;   // largest bound on the symbolic CTA table
   int warp_log_max;    // log2 of the largest warp table
   float max_load;      // numeric table load factor
+  // numeric / learned binning: rows with more than block_min entries go to
+  // the CTA-wide hash bins (kBinBlock up to blk_small_cap entries, kBinDense
+  // up to blk_large_cap); block_min = INT64_MAX and the caps 0 turn them off
+  int64_t block_min;
+  int64_t blk_small_cap;
+  int64_t blk_large_cap;
 };
+
+// BinParams with the CTA-wide numeric bins turned off (paths that only
+// launch the warp bins and the heavy tiles).
+inline BinParams without_block_bins(BinParams bp) {
+  bp.block_min = INT64_MAX;
+  bp.blk_small_cap = 0;
+  bp.blk_large_cap = 0;
+  return bp;
+}
 
 struct LaunchCtx {
   cudaStream_t stream;
@@ -71,6 +90,14 @@ void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int3
                              const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
                              int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
                              const LaunchCtx& lc, int wpb);
+// CTA-wide hash numeric pass over the rows of bin kBinBlock (2^12-slot
+// tables) or kBinDense (2^14) of a numeric / learned binning.
+void launch_num_block(int bin, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, const int64_t* c_rp,
+                      int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc);
+void launch_num_block_learned(int bin, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
+                              const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
+                              int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
+                              const LaunchCtx& lc);
 // Copies n 32-bit words with one small kernel (dst may be mapped pinned host
 // memory: the read-back then needs no copy engine).
 void launch_copy_words(const void* src, void* dst, int64_t n, const LaunchCtx& lc);

@@ -292,10 +292,12 @@ __global__ void __launch_bounds__(kPlanWarps * 32) k_mlp_predict(const __nv_bflo
 
 // Capacity from a prediction: cap = min(bound, ceil(margin * (2^o0 - 1)) +
 // slack); a row goes to the exact path (need_exact = 1, cap = 0) when its
-// cap exceeds the largest warp table or its predicted bin says heavy;
-// force_overflow sets cap = 1 (every row then overflows and is re-run).
+// cap exceeds the largest table of the learned pass (learn_cap) or, with
+// bin_gate, its predicted bin says beyond the warp tables; force_overflow
+// sets cap = 1 (every row then overflows and is re-run).
 __device__ __forceinline__ void capacity_of(int64_t p, int64_t cols, float o0, float o1, float margin, int slack,
-                                            int64_t warp_cap, int force_overflow, int64_t& cap, uint8_t& ex) {
+                                            int64_t learn_cap, int bin_gate, int force_overflow, int64_t& cap,
+                                            uint8_t& ex) {
   const int64_t u = p < cols ? p : cols;
   cap = 0;
   ex = 0;
@@ -306,7 +308,7 @@ __device__ __forceinline__ void capacity_of(int64_t p, int64_t cols, float o0, f
   int64_t c = cd >= (double)u ? u : (int64_t)cd;
   if (c < 1) c = 1;
   if (force_overflow) c = 1;
-  if (c > warp_cap || o1 > (float)kMaxLogT + 0.5f) {
+  if (c > learn_cap || (bin_gate && o1 > (float)kMaxLogT + 0.5f)) {
     ex = 1;
     c = 0;
   }
@@ -320,8 +322,9 @@ __device__ __forceinline__ void capacity_of(int64_t p, int64_t cols, float o0, f
 // rows marked for the exact path.
 template <bool R32>
 __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B, const __nv_bfloat16* w,
-                                                                  float margin, int slack, int64_t warp_cap,
-                                                                  int force_overflow, int64_t* prod, int64_t* cap,
+                                                                  float margin, int slack, int64_t learn_cap,
+                                                                  int bin_gate, int force_overflow, int64_t* prod,
+                                                                  int64_t* cap,
                                                                   uint8_t* need_exact,
                                                                   unsigned long long* n_exact) {
   __shared__ MlpSmem sm;
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B
       if (ra < rows) {
         int64_t c;
         uint8_t ex;
-        capacity_of(tprod[wib][ia], B.cols, o[0], o[1], margin, slack, warp_cap, force_overflow, c, ex);
+        capacity_of(tprod[wib][ia], B.cols, o[0], o[1], margin, slack, learn_cap, bin_gate, force_overflow, c, ex);
         prod[ra] = tprod[wib][ia];
         cap[ra] = c;
         need_exact[ra] = ex;
@@ -367,7 +370,7 @@ __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B
       if (rb < rows) {
         int64_t c;
         uint8_t ex;
-        capacity_of(tprod[wib][ib], B.cols, o[2], o[3], margin, slack, warp_cap, force_overflow, c, ex);
+        capacity_of(tprod[wib][ib], B.cols, o[2], o[3], margin, slack, learn_cap, bin_gate, force_overflow, c, ex);
         prod[rb] = tprod[wib][ib];
         cap[rb] = c;
         need_exact[rb] = ex;
@@ -572,20 +575,20 @@ void launch_mlp_predict(const void* w16, const float* feats, int64_t rows, float
   k_mlp_predict<<<blocks, kPlanWarps * 32, 0, lc.stream>>>((const __nv_bfloat16*)w16, feats, rows, out);
 }
 
-void launch_learned_plan(const DCsr& A, const DCsr& B, const void* w16, float margin, int slack, int64_t warp_cap,
-                         int force_overflow, int64_t* prod, int64_t* cap, uint8_t* need_exact,
+void launch_learned_plan(const DCsr& A, const DCsr& B, const void* w16, float margin, int slack, int64_t learn_cap,
+                         int bin_gate, int force_overflow, int64_t* prod, int64_t* cap, uint8_t* need_exact,
                          unsigned long long* n_exact, const LaunchCtx& lc) {
   if (A.rows == 0) return;
   const int64_t tiles = (A.rows + 15) / 16;
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((tiles + kPlanWarps - 1) / kPlanWarps, lc.sms * 8));
   if (B.rp32)
     k_learned_plan<true><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(A, B, (const __nv_bfloat16*)w16, margin, slack,
-                                                                    warp_cap, force_overflow, prod, cap, need_exact,
-                                                                    n_exact);
+                                                                    learn_cap, bin_gate, force_overflow, prod, cap,
+                                                                    need_exact, n_exact);
   else
     k_learned_plan<false><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(A, B, (const __nv_bfloat16*)w16, margin, slack,
-                                                                     warp_cap, force_overflow, prod, cap, need_exact,
-                                                                     n_exact);
+                                                                     learn_cap, bin_gate, force_overflow, prod, cap,
+                                                                     need_exact, n_exact);
 }
 
 void launch_mlp_fwd_bwd(const void* w16, const float* feats, const float* targets, int64_t n, float* work,

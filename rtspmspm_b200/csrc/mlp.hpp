@@ -15,9 +15,11 @@ constexpr int kMlpParams = kMlpIn * kMlpHidden + kMlpHidden + kMlpHidden * kMlpH
 
 void launch_features(const DCsr& A, const DCsr& B, float* feats, int64_t* prod, const LaunchCtx& lc);
 void launch_mlp_predict(const void* w16, const float* feats, int64_t rows, float* out, const LaunchCtx& lc);
-// Fused learned plan: per row products, MLP capacity and exact-path mark.
-void launch_learned_plan(const DCsr& A, const DCsr& B, const void* w16, float margin, int slack, int64_t warp_cap,
-                         int force_overflow, int64_t* prod, int64_t* cap, uint8_t* need_exact,
+// Fused learned plan: per row products, MLP capacity and exact-path mark
+// (capacity above learn_cap, or with bin_gate a predicted bin beyond the
+// warp tables).
+void launch_learned_plan(const DCsr& A, const DCsr& B, const void* w16, float margin, int slack, int64_t learn_cap,
+                         int bin_gate, int force_overflow, int64_t* prod, int64_t* cap, uint8_t* need_exact,
                          unsigned long long* n_exact, const LaunchCtx& lc);
 // Forward + backward over n rows; `work` holds mlp_work_floats(n) floats;
 // grad gets the full gradient (overwritten); loss (device) the mean loss.

@@ -178,7 +178,8 @@ extern "C" spg_status spg_multiply_noalloc(void* stream, const spg_csr* A, const
     return err(errbuf, errlen, SPG_ERR_INVALID_ARG,
                "input failed validation (index out of range, unsorted or duplicate columns, bad row pointers)");
 
-  const BinParams bp = bin_params(default_tuning());
+  // the warp bins only (rows above them are rejected)
+  const BinParams bp = without_block_bins(bin_params(default_tuning()));
   const int wpb = default_tuning().warps_per_block;
   launch_row_products(dA, dB, prod, lc);
   launch_binning(prod, rows, B->cols, kBinSymbolic, bp, bins, counts, offsets, cursors, lists, lc);

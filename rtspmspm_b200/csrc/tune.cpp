@@ -132,6 +132,8 @@ spg_status spg_set_tuning(spg_ctx* ctx, const spg_tuning* in) {
   if (t.predict_slack < 0) t.predict_slack = d.predict_slack;
   if (!(t.learned_load > 0.05f && t.learned_load < 0.95f)) t.learned_load = d.learned_load;
   if (t.heavy_path != 0 && t.heavy_path != 1) return fail(ctx, SPG_ERR_INVALID_ARG, "heavy_path must be 0 or 1");
+  if (t.block_min_nnz > (1 << kBlkLogLargeT) / 2)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "block_min_nnz above the largest CTA table (use -1 to turn the CTA bins off)");
   ctx->tuning = t;
   return SPG_OK;
 }

@@ -28,10 +28,15 @@ def ref(name, A, B):
 # tunings that push rows onto every accumulator kind
 TUNINGS = {
     "default": {},
-    "tiny_tables": {"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5},
+    # CTA hash bins off: rows beyond 32 entries go to the heavy-row tiles
+    "tiny_tables": {"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5, "block_min_nnz": -1},
+    # rows beyond 166 entries in the CTA hash bins
     "mid_tables": {"warp_table_max": 256, "block_table_max": 2048, "max_load": 0.65, "warps_per_block": 4},
     # heavy rows through the staged per-tile buckets instead of the rescanning tile kernel
-    "tiny_staged": {"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5, "heavy_path": 1},
+    "tiny_staged": {"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5, "heavy_path": 1,
+                    "block_min_nnz": -1},
+    # every row of more than 8 entries in a CTA hash bin
+    "cta_bins": {"block_min_nnz": 8},
 }
 
 
@@ -40,7 +45,7 @@ TUNINGS = {
 @pytest.mark.parametrize("name,A,B", PAIRS, ids=[p[0] for p in PAIRS])
 def test_parity(engine, name, A, B, algo, tuning):
     engine.set_tuning(**{**{"warp_table_max": 4096, "block_table_max": 16384, "max_load": 0.5,
-                            "warps_per_block": 8, "heavy_path": 0}, **TUNINGS[tuning]})
+                            "warps_per_block": 8, "heavy_path": 0, "block_min_nnz": 0}, **TUNINGS[tuning]})
     C, rep = engine.multiply(A, B, algo=algo, use_tuning=True, stage_timing=True)
     R = ref(name, A, B)
     assert_parity(C.to_host(), R)

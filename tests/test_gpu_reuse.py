@@ -40,18 +40,22 @@ def test_reuse_matches_oracle_on_new_values(engine, name, bits):
         C.free()
 
 
-@pytest.mark.parametrize("tuning", [{"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5},
-                                    {"warp_table_max": 4096}])
-def test_reuse_heavy_rows(tuning):
+@pytest.mark.parametrize("tuning,heavy", [
+    ({"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5, "block_min_nnz": -1}, True),
+    ({"warp_table_max": 4096, "block_min_nnz": -1}, True),
+    ({"warp_table_max": 4096, "block_min_nnz": 8}, False)])
+def test_reuse_heavy_rows(tuning, heavy):
     """Rows beyond the warp tables take the column-tile path (tile counts
-    read from C's columns)."""
+    read from C's columns) or, with the CTA hash bins on, the CTA tables."""
     eng = Engine(0)
     try:
         eng.set_tuning(**tuning)
         for A in (heavy_row(), gen.rmat(13, 16, seed=3)):
             dA = DeviceCsr.from_host(A)
             C, rep = eng.multiply(dA, dA, algo="plain", use_tuning=True)
-            assert rep["rows_heavy"] > 0
+            assert (rep["rows_heavy"] > 0) == heavy
+            if not heavy:
+                assert rep["bin_rows"][8] + rep["bin_rows"][9] > 0
             A2 = revalue(A, 5)
             eng.multiply_reuse(A2, A2, C, use_tuning=True)
             assert_parity(C.to_host(), oracle.spgemm(A2, A2))

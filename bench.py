@@ -354,23 +354,26 @@ def measure_batch(eng, pairs, warmup, steps, flush, stream, tune=True, modes=Non
         eng.tune(dA[:min(64, len(dA))], dB[:min(64, len(dB))], None)
         out["tune_s"] = round(time.perf_counter() - t, 2)
         out["tuning"] = eng.get_tuning()
-    for graph, tuned in modes or ((True, True), (False, True), (True, False)):
+    for graph, tuned, algo in modes or ((True, True, "plain"), (False, True, "plain"), (True, False, "plain"),
+                                        (True, False, "learned")):
         if tuned and not tune:
             continue
         for _ in range(warmup):
-            eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True)
+            eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True, algo=algo)
         holder = {}
 
         def step():
-            res, rep = eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True)
+            res, rep = eng.multiply_batched(dA, dB, use_graph=graph, use_tuning=tuned, skip_validation=True,
+                                            algo=algo)
             holder["rep"] = rep
 
         ms = timed_median(step, steps, flush, stream)
-        key = ("graph" if graph else "stream") + ("_tuned" if tuned else "_default")
+        key = ("graph" if graph else "stream") + ("_tuned" if tuned else "_default") + \
+            ("_learned" if algo == "learned" else "")
         rep = holder["rep"]
         out[key] = {"ms": round(ms, 3), "gflops": round(2 * products / ms / 1e6, 2), "nnz_c": rep["nnz_c"],
-                    "kernel_launches": rep["kernel_launches"], "rows_overflow": rep.get("rows_overflow", 0),
-                    "products_individual": rep.get("rows_heavy", 0)}
+                    "kernel_launches": rep["kernel_launches"], "rows_predicted": rep.get("rows_predicted", 0),
+                    "rows_overflow": rep.get("rows_overflow", 0), "products_individual": rep.get("rows_heavy", 0)}
     del dA, dB
     return out
 
@@ -420,7 +423,10 @@ def extra_workloads(args, eng, flush, stream) -> dict:
                                    stream)
     pairs = gen.batch_uneven(count=512, seed=1)
     out["batch512"] = measure_batch(eng, pairs, 3, max(3, min(args.steps, 10)), flush, stream,
-                                    modes=((True, True), (True, False)))
+                                    modes=((True, True, "plain"), (True, False, "plain"), (True, False, "learned")))
+    b = out["batch512"]
+    if "graph_default" in b and "graph_default_learned" in b:
+        b["speedup_learned_vs_plain"] = round(b["graph_default"]["ms"] / b["graph_default_learned"]["ms"], 4)
     del pairs
     A = gen.rmat(20, 16, seed=0)
     out["rmat20"] = measure_single(eng, A, ["plain", "learned"], 1, 3, flush, stream)

@@ -3,18 +3,21 @@
 // No reference counterpart: the reference runs one product per process
 // (scripts/AE_test.py:199-215).  Here all rows of all products form one
 // global row space, binned by table size across every matrix at once; each
-// stage (symbolic, numeric) is one launch per warp-table size whose warps
-// stride over that bin's rows of all products, so small and large products
-// share the GPU without per-matrix launches.  Bin bounds are read on the
-// device, and the launch sequence is captured once into a CUDA graph and
-// replayed while the inputs stay the same.
+// stage (symbolic, numeric) is two persistent launches that drain a queue of
+// (bin, row range) tiles of all products -- one queue of small warp tables,
+// whose CTAs stay small so that many share an SM, and one of large warp
+// tables plus a CTA-wide table for the largest rows -- so small and large
+// products share the GPU without per-matrix or per-bin launches.  Bin bounds
+// and tile counts are derived on the device, and the launch sequence is
+// captured once into a CUDA graph and replayed while the inputs stay the
+// same.
 //
 // Plan (host, once per input set): matrix descriptors, global-row -> matrix
 // map, the nnz upper bound of every product (sum over rows of
 // min(products, cols)), so that every C_m gets a fixed region of one output
 // slab and no host round trip is needed while the graph runs.
-// Products whose bound exceeds the warp tables are run one by one through
-// the single-product path instead.
+// Products with a row of more than kBatchMaxBound products (capped at the
+// columns) are run one by one through the single-product path instead.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,24 +25,13 @@
 #include <memory>
 #include <vector>
 
+#include "block_row.cuh"
 #include "context.hpp"
 #include "warp_row.cuh"
 
 using namespace spg;
 
 namespace spg {
-
-struct BatchMat {
-  DCsr A;
-  DCsr B;
-  int64_t row_start;  // first global row of this product
-  int64_t c_base;     // first entry of C_m in the output slab
-  int64_t rp_base;    // first entry of C_m's row pointers in the row-pointer slab
-};
-
-// Largest CTA of the per-bin kernels: 8 warps, tables within 200 KB.
-constexpr int kBatchWarps = 8;
-constexpr int kBatchCtaTableBytes = 200 * 1024;
 
 // Products per global row and the bound min(products, cols_m).
 __global__ void k_batch_products(const BatchMat* mats, const int32_t* row_mat, int64_t R, int64_t* prod,
@@ -77,37 +69,66 @@ __global__ void k_batch_bound_stats(const int32_t* row_mat, const int64_t* bound
   }
 }
 
-// Shared-memory bytes a warp's table takes: 2^logt slots of keys when
-// symbolic; keys, values and the first-seen list when numeric.
-inline size_t batch_table_bytes(int logt, bool numeric) { return ((size_t)1 << logt) * (numeric ? 12 : 4); }
+// One persistent launch drains a queue of tiles -- runs of rows of one bin,
+// all products mixed -- in the order the queue lists its bins (largest rows
+// first).  A queue holds either warp bins only (each warp of the CTA takes
+// rows of the tile with its own table of 2^L slots) or also the CTA bin
+// (kBinBlock: the CTA takes the tile's rows one at a time with one CTA-wide
+// table of 2^CTA_LOGT slots, block_row.cuh).  The tile count of every bin is
+// derived on the device from the binning's offsets (k_queue_prefix), so the
+// launch needs no host round trip and replays from a CUDA graph.
+constexpr int kQueueMax = 8;
 
-// Symbolic (NUMERIC = false) or numeric (true) pass over the rows of warp
-// bin LOGT of the global row space: warp per row, rows taken in stride from
-// the bin's list (its bounds read from bin_off on the device, so the launch
-// needs no host round trip and replays from a graph).  Each row looks up its
-// product's descriptor.  Tables are epoch-tagged while the product's B has
-// fewer than 2^24 columns; a row of a wider product clears the table first
-// if tagged keys may be left in it.
-template <int LOGT, bool NUMERIC>
-__global__ void __launch_bounds__(512, 2) k_batch_bin(const BatchMat* mats, const int32_t* row_mat,
-                                                      const int32_t* lists, const int64_t* bin_off, int64_t* nnz,
-                                                      const int64_t* gscan, int32_t* c_col, float* c_val,
-                                                      int* flags) {
+struct BatchQueue {
+  int nq;                          // bins in this queue
+  int bins[kQueueMax];             // bin per queue slot
+  int rows_per_tile[kQueueMax];
+};
+
+// tile_pref[i] = tiles of queue slots before i (tile_pref[nq] = all).
+__global__ void k_queue_prefix(const int64_t* bin_off, BatchQueue q, int64_t* tile_pref) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int64_t t = 0;
+    for (int i = 0; i < q.nq; ++i) {
+      tile_pref[i] = t;
+      const int64_t rows = bin_off[q.bins[i] + 1] - bin_off[q.bins[i]];
+      t += (rows + q.rows_per_tile[i] - 1) / q.rows_per_tile[i];
+    }
+    tile_pref[q.nq] = t;
+  }
+}
+
+// Outputs of the learned numeric pass: each predicted row is written sorted
+// into its slab slot (slab_off[g], capacity cap[g]); a row with more columns
+// than its capacity is queued in retry for the exact re-run (nnz[g] = -1).
+struct LearnedOut {
+  const int64_t* cap;
+  const int64_t* slab_off;
+  int32_t* slab_col;
+  float* slab_val;
+  int32_t* retry;
+  unsigned long long* retry_count;
+};
+
+// One warp over rows [first, last) of a warp bin of table 2^LOGT (its slot
+// `sm`, of the size of the queue's largest table).  Tables are epoch-tagged
+// while the product's B has fewer than 2^24 columns; a row of a wider product
+// clears the table first if tagged keys may be left in it.
+template <int LOGT, bool NUMERIC, bool LEARNED>
+__device__ __forceinline__ void warp_tile(const BatchMat* mats, const int32_t* row_mat, const int32_t* lists,
+                                          int64_t first, int64_t last, int32_t* sm, int64_t* nnz,
+                                          const int64_t* gscan, int32_t* c_col, float* c_val, const LearnedOut& lo,
+                                          int* flags) {
   constexpr int T = 1 << LOGT;
-  constexpr int kWords = NUMERIC ? numeric_words<LOGT>() : T;
-  extern __shared__ int32_t sm_tab[];
   const int lane = lane_id();
-  int32_t* keys = sm_tab + (threadIdx.x >> 5) * kWords;
+  int32_t* keys = sm;
   float* vals = reinterpret_cast<float*>(keys + T);
   int32_t* list = keys + 2 * T;
   for (int s2 = lane; s2 < T; s2 += 32) keys[s2] = kEmpty;
   __syncwarp();
-  const int64_t first = bin_off[LOGT - kMinLogT], last = bin_off[LOGT - kMinLogT + 1];
-  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   int epoch = 0;
   bool tagged = false;  // keys of an epoch may be in the table
-  for (int64_t i = first + gw; i < last; i += nw) {
+  for (int64_t i = first; i < last; ++i) {
     const int64_t g = lists[i];
     const BatchMat& M = mats[row_mat[g]];
     const int32_t r = (int32_t)(g - M.row_start);
@@ -124,18 +145,145 @@ __global__ void __launch_bounds__(512, 2) k_batch_bin(const BatchMat* mats, cons
     if (!NUMERIC) {
       const int cnt = symbolic_row<LOGT, true>(M.A, M.B, r, keys, ep, flags);
       if (lane == 0) nnz[g] = cnt;
+    } else if (LEARNED) {
+      const int n = accumulate_row<LOGT, true, true>(M.A, M.B, r, keys, vals, list, ep, (int)lo.cap[g], flags);
+      if (n < 0) {
+        if (lane == 0) {
+          nnz[g] = -1;
+          lo.retry[atomicAdd(lo.retry_count, 1ull)] = (int32_t)g;
+        }
+      } else {
+        const int64_t off = lo.slab_off[g];
+        emit_row<LOGT>(keys, vals, list, n, ep, n, lo.slab_col + off, lo.slab_val + off, false);
+        if (lane == 0) nnz[g] = n;
+      }
     } else {
-      const int64_t base = gscan[M.row_start];
-      const int64_t off = M.c_base + (gscan[g] - base);
+      const int64_t off = M.c_base + (gscan[g] - gscan[M.row_start]);
       numeric_row<LOGT, true, true>(M.A, M.B, r, keys, vals, list, ep, c_col + off, c_val + off,
                                     gscan[g + 1] - gscan[g], flags);
     }
+    if (LEARNED && ep < 0) next_row<LOGT>(keys, ep);  // plain keys: cleared after every row
     if (ep >= 0) {
       tagged = true;
-      if (!NUMERIC) next_row<LOGT>(keys, ep);
+      if (!NUMERIC || LEARNED) next_row<LOGT>(keys, ep);
       epoch = ep;
       if (epoch == 0) tagged = false;  // wiped on wrap
     }
+  }
+}
+
+// Tile t of queue q: its bin and rows [first, last) of the bin's list.
+__device__ __forceinline__ int decode_tile(const BatchQueue& q, const int64_t* tile_pref, const int64_t* bin_off,
+                                           int64_t t, int64_t& first, int64_t& last) {
+  int qi = 0;
+  while (qi + 1 < q.nq && tile_pref[qi + 1] <= t) ++qi;
+  const int b = q.bins[qi];
+  first = bin_off[b] + (t - tile_pref[qi]) * q.rows_per_tile[qi];
+  last = min(bin_off[b + 1], first + q.rows_per_tile[qi]);
+  return b;
+}
+
+// Persistent symbolic (NUMERIC = false: exact nnz per row into nnz) or
+// numeric (rows written into the output slab at gscan) pass over the queue
+// q: warp bins of tables 2^LMIN..2^LMAX and, when CTA_LOGT > 0, the CTA bin,
+// which the queue lists first.  CTA-bin tiles are taken by whole CTAs (one
+// ticket per CTA); the first warp-bin tile a CTA draws goes to its warp 0
+// and from then on every warp takes its own tickets, so warps working on
+// rows of different sizes never wait for one another.  (MINB: CTAs per SM
+// the registers must allow.)
+template <bool NUMERIC, bool LEARNED, int LMIN, int LMAX, int CTA_LOGT, int MINB>
+__global__ void __launch_bounds__(kBlkThreads, MINB) k_batch_queue(const BatchMat* mats, const int32_t* row_mat,
+                                                                   const int32_t* lists, const int64_t* bin_off,
+                                                                   BatchQueue q, const int64_t* tile_pref,
+                                                                   const int64_t* bound, int64_t* nnz,
+                                                                   const int64_t* gscan, int32_t* c_col,
+                                                                   float* c_val, LearnedOut lo,
+                                                                   unsigned long long* counter, int* flags) {
+  extern __shared__ int32_t sm_q[];
+  __shared__ unsigned long long sh_tile;
+  const int tid = threadIdx.x, lane = lane_id(), wib = tid >> 5;
+  const int64_t ntiles = tile_pref[q.nq];
+  int64_t handed = -1;  // a warp-bin tile drawn in CTA mode, for warp 0
+  if (CTA_LOGT > 0) {
+    constexpr int CL = CTA_LOGT > 0 ? CTA_LOGT : 1;
+    constexpr int TC = 1 << CL;
+    int32_t* keys = sm_q;
+    float* vals = reinterpret_cast<float*>(sm_q + TC);
+    uint32_t* own = reinterpret_cast<uint32_t*>(sm_q + 2 * TC);
+    BlockScratch& sc = *reinterpret_cast<BlockScratch*>(sm_q + (NUMERIC ? 3 * TC : TC));
+    for (;;) {
+      if (tid == 0) sh_tile = atomicAdd(counter, 1ull);
+      __syncthreads();
+      const int64_t t = (int64_t)sh_tile;
+      __syncthreads();  // read by every thread before the next ticket
+      if (t >= ntiles) return;
+      int64_t first, last;
+      const int b = decode_tile(q, tile_pref, bin_off, t, first, last);
+      if (b != kBinBlock) {
+        handed = t;
+        break;
+      }
+      for (int64_t i = first; i < last; ++i) {
+        const int64_t g = lists[i];
+        const BatchMat& M = mats[row_mat[g]];
+        const int32_t r = (int32_t)(g - M.row_start);
+        if (LEARNED) {
+          const int64_t c = lo.cap[g];
+          const int lg = cta_table_log(c, CL);
+          const int n = cta_accumulate_row<CL, true, true>(M.A, M.B, r, keys, vals, own, sc, c, flags, lg);
+          if (n < 0) {
+            if (tid == 0) {
+              nnz[g] = -1;
+              lo.retry[atomicAdd(lo.retry_count, 1ull)] = (int32_t)g;
+            }
+          } else {
+            const int64_t off = lo.slab_off[g];
+            cta_emit_row<CL>(keys, vals, own, sc, n, n, lo.slab_col + off, lo.slab_val + off, lg);
+            if (tid == 0) nnz[g] = n;
+          }
+        } else if (NUMERIC) {
+          const int64_t off = M.c_base + (gscan[g] - gscan[M.row_start]);
+          const int64_t want = gscan[g + 1] - gscan[g];
+          const int lg = cta_table_log(want, CL);
+          const int n = cta_accumulate_row<CL, true, false>(M.A, M.B, r, keys, vals, own, sc, 0, flags, lg);
+          if (n != want && tid == 0) raise_flag(flags, kFlagCountDiff);
+          cta_emit_row<CL>(keys, vals, own, sc, n, want, c_col + off, c_val + off, lg);
+        } else {
+          // symbolic: the table sized from the row's bound (products capped at the columns)
+          const int lg = cta_table_log(bound[g], CL);
+          const int n = cta_accumulate_row<CL, true, false, false>(M.A, M.B, r, keys, vals, own, sc, 0, flags, lg);
+          if (tid == 0) nnz[g] = n;
+        }
+      }
+    }
+    __syncthreads();  // the CTA table's memory becomes the warps' tables
+  }
+  // warp mode: each warp its own tickets and table slot
+  int32_t* slot = sm_q + (size_t)wib * (NUMERIC ? numeric_words<LMAX>() : (1 << LMAX));
+  for (;;) {
+    int64_t t;
+    if (wib == 0 && handed >= 0) {
+      t = handed;
+      handed = -1;
+    } else {
+      unsigned long long x = 0;
+      if (lane == 0) x = atomicAdd(counter, 1ull);
+      t = (int64_t)__shfl_sync(kFull, x, 0);
+    }
+    if (t >= ntiles) break;
+    int64_t first, last;
+    const int b = decode_tile(q, tile_pref, bin_off, t, first, last);
+    if (b == kBinBlock) {  // cannot happen: the CTA bin comes first in the queue
+      if (lane == 0) raise_flag(flags, kFlagHashFull);
+      continue;
+    }
+    const int L = kMinLogT + b;
+#define SPG_WT(LL)                                                                                          \
+  if (L == LL && LL >= LMIN && LL <= LMAX)                                                                  \
+    warp_tile<(LL >= LMIN && LL <= LMAX) ? LL : LMIN, NUMERIC, LEARNED>(mats, row_mat, lists, first, last, slot, \
+                                                                        nnz, gscan, c_col, c_val, lo, flags);
+    SPG_WT(5) SPG_WT(6) SPG_WT(7) SPG_WT(8) SPG_WT(9) SPG_WT(10) SPG_WT(11)
+#undef SPG_WT
   }
 }
 
@@ -158,7 +306,124 @@ __global__ void k_batch_finalize(const BatchMat* mats, int n, const int32_t* row
   }
 }
 
+// Learned batch: copies every predicted row that did not overflow
+// (need[g] == 0) from its slab slot to its place in C (warp per row).
+__global__ void k_batch_compact(const BatchMat* mats, const int32_t* row_mat, int64_t R, const uint8_t* need,
+                                const int64_t* slab_off, const int32_t* slab_col, const float* slab_val,
+                                const int64_t* gscan, int32_t* c_col, float* c_val) {
+  const int lane = lane_id();
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t g = gw; g < R; g += nw) {
+    if (need[g]) continue;
+    const BatchMat& M = mats[row_mat[g]];
+    const int64_t n = gscan[g + 1] - gscan[g];
+    const int64_t src = slab_off[g];
+    const int64_t dst = M.c_base + (gscan[g] - gscan[M.row_start]);
+    for (int64_t t = lane; t < n; t += 32) {
+      c_col[dst + t] = slab_col[src + t];
+      c_val[dst + t] = slab_val[src + t];
+    }
+  }
+}
+
 namespace {
+
+// The queue launches: symbolic small / large tables, numeric small / mid /
+// large tables (the numeric ones also in a learned form).  Warp-only queues
+// size their CTAs for their largest warp table, so small tables keep many
+// warps per SM; the large queues hold the CTA bin.
+constexpr int kQueues = 5;
+constexpr int kQSymSmall = 0, kQSymLarge = 1, kQNumSmall = 2, kQNumMid = 3, kQNumLarge = 4;
+// Rows of more than kBatchMaxBound products (capped at the columns) are
+// beyond the queue's tables: their products run one by one instead.
+constexpr int64_t kBatchMaxBound = 4096;
+constexpr int kBatchCtaLogT = 13;  // CTA tables: 2^13 slots at load <= 1/2
+
+BatchQueue queue_of(int which) {
+  BatchQueue q{};
+  auto add = [&](int bin, int rpt) {
+    q.bins[q.nq] = bin;
+    q.rows_per_tile[q.nq] = rpt;
+    ++q.nq;
+  };
+  switch (which) {
+    case kQSymSmall:
+      for (int l = 10; l >= 5; --l) add(l - kMinLogT, l >= 9 ? 2 : 8);
+      break;
+    case kQSymLarge:
+      add(kBinBlock, 1);
+      add(11 - kMinLogT, 1);
+      break;
+    case kQNumSmall:
+      for (int l = 9; l >= 5; --l) add(l - kMinLogT, l >= 8 ? 2 : 8);
+      break;
+    case kQNumMid:
+      add(10 - kMinLogT, 1);
+      break;
+    default:
+      add(kBinBlock, 1);
+      break;
+  }
+  return q;
+}
+
+// Dynamic shared memory of a queue launch: one table slot of the queue's
+// largest warp table per warp, or the CTA table and its scratch.
+size_t queue_smem(int which) {
+  const size_t sc = sizeof(BlockScratch);
+  switch (which) {
+    case kQSymSmall: return (size_t)kBlkWarps * 4 * (1 << 10);
+    case kQSymLarge: return std::max((size_t)kBlkWarps * 4 * (1 << 11), (size_t)4 * (1 << kBatchCtaLogT) + sc);
+    case kQNumSmall: return (size_t)kBlkWarps * 12 * (1 << 9);
+    case kQNumMid: return (size_t)kBlkWarps * 12 * (1 << 10);
+    default: return (size_t)12 * (1 << kBatchCtaLogT) + sc;
+  }
+}
+
+// The kernel of queue `which` (the learned form of a numeric queue when
+// `learned`) and, with `args`, its launch.
+struct QueueArgs {
+  const BatchMat* mats;
+  const int32_t* row_mat;
+  const int32_t* lists;
+  const int64_t* bin_off;
+  BatchQueue q;
+  const int64_t* tile_pref;
+  const int64_t* bound;
+  int64_t* nnz;
+  const int64_t* gscan;
+  int32_t* c_col;
+  float* c_val;
+  LearnedOut lo;
+  unsigned long long* counter;
+  int* flags;
+};
+
+template <bool NUMERIC, bool LEARNED, int LMIN, int LMAX, int CTA, int MINB>
+const void* queue_launch(const QueueArgs* a, int grid, size_t smem, cudaStream_t st) {
+  auto k = k_batch_queue<NUMERIC, LEARNED, LMIN, LMAX, CTA, MINB>;
+  if (a)
+    k<<<grid, kBlkThreads, smem, st>>>(a->mats, a->row_mat, a->lists, a->bin_off, a->q, a->tile_pref, a->bound,
+                                       a->nnz, a->gscan, a->c_col, a->c_val, a->lo, a->counter, a->flags);
+  return (const void*)k;
+}
+
+const void* queue_dispatch(int which, bool learned, const QueueArgs* a, int grid, size_t smem, cudaStream_t st) {
+  switch (which) {
+    case kQSymSmall: return queue_launch<false, false, 5, 10, 0, 4>(a, grid, smem, st);
+    case kQSymLarge: return queue_launch<false, false, 11, 11, kBatchCtaLogT, 2>(a, grid, smem, st);
+    case kQNumSmall:
+      return learned ? queue_launch<true, true, 5, 9, 0, 4>(a, grid, smem, st)
+                     : queue_launch<true, false, 5, 9, 0, 4>(a, grid, smem, st);
+    case kQNumMid:
+      return learned ? queue_launch<true, true, 10, 10, 0, 2>(a, grid, smem, st)
+                     : queue_launch<true, false, 10, 10, 0, 2>(a, grid, smem, st);
+    default:
+      return learned ? queue_launch<true, true, 10, 10, kBatchCtaLogT, 2>(a, grid, smem, st)
+                     : queue_launch<true, false, 10, 10, kBatchCtaLogT, 2>(a, grid, smem, st);
+  }
+}
 
 struct BatchPlan {
   std::vector<uintptr_t> key;
@@ -186,8 +451,22 @@ struct BatchPlan {
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
   spg_tuning tune{};
-  int per_sm[2][kNumWarpBins] = {};  // CTAs per SM of the per-bin kernels (symbolic, numeric)
-  int warps[2][kNumWarpBins] = {};   // warps per CTA of the per-bin kernels
+  BinParams bp_sym{}, bp_num{}, bp_lrn{};  // binnings: symbolic, numeric, learned
+  int grid[2][kQueues] = {};               // CTAs of each queue launch (plain, learned form)
+  int64_t* tile_pref = nullptr;            // kQueues x (kQueueMax + 1)
+  unsigned long long* qcount = nullptr;    // tile tickets, kQueues
+  // learned method
+  bool learned = false;
+  int force_overflow = 0;
+  int64_t* cap = nullptr;        // R + 1 predicted capacities
+  int64_t* slab_off = nullptr;   // R + 1
+  uint8_t* need = nullptr;       // rows on the exact path
+  int64_t* mkey = nullptr;       // R masked sizes
+  int32_t* retry = nullptr;      // overflowed rows
+  int32_t* slab_col = nullptr;
+  float* slab_val = nullptr;
+  unsigned long long* lcount = nullptr;  // [0] rows predicted heavy, [1] overflowed rows
+  unsigned long long* h_lcount = nullptr;  // pinned copy
   int launches = 0;
 };
 
@@ -197,6 +476,7 @@ void free_plan(BatchPlan* p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   for (void* q : p->owned) cudaFree(q);
   if (p->h_nnz_m) cudaFreeHost(p->h_nnz_m);
+  if (p->h_lcount) cudaFreeHost(p->h_lcount);
   delete p;
 }
 
@@ -217,6 +497,8 @@ std::vector<uintptr_t> plan_key(spg_ctx* ctx, int n, const spg_csr* A, const spg
   k.push_back((uintptr_t)t.warp_table_max);
   k.push_back((uintptr_t)(t.max_load * 1000.0f));
   k.push_back((uintptr_t)t.warps_per_block);
+  k.push_back((uintptr_t)(t.learned_load * 1000.0f));
+  k.push_back((uintptr_t)(o.algo == SPG_ALGO_LEARNED ? 1 + (o.force_overflow ? 1 : 0) : 0));
   for (int m = 0; m < n; ++m) {
     for (const spg_csr* x : {&A[m], &B[m]}) {
       k.push_back((uintptr_t)x->row_ptr);
@@ -231,9 +513,15 @@ std::vector<uintptr_t> plan_key(spg_ctx* ctx, int n, const spg_csr* A, const spg
 }
 
 // Issues the device work of one batched execution on ctx->stream.
+// Plain: bounds, symbolic binning, the symbolic queues, numeric binning and
+// scan, the numeric queues, per-product row pointers.  Learned: the batched
+// plan (products, features, tensor-core MLP capacity), learned binning, the
+// learned numeric queues into a capacity-sized slab; rows predicted beyond
+// the tables or overflowed go through the symbolic and numeric queues
+// exactly (empty queues when there are none, so no host round trip is
+// needed), the scan of the final sizes, the slab rows copied into C.
 void enqueue(spg_ctx* ctx, BatchPlan* p) {
   const LaunchCtx lc = launch_ctx(ctx);
-  const BinParams bp = without_block_bins(bin_params(p->tune));
   int launches = 0;
   const int64_t R = p->R;
   auto blocks_for = [&](int64_t work, int per_block) {
@@ -246,38 +534,74 @@ void enqueue(spg_ctx* ctx, BatchPlan* p) {
   int64_t* counts = p->binmeta;
   int64_t* offsets = p->binmeta + kNumBins;
   int64_t* cursors = p->binmeta + 2 * kNumBins + 1;
-  launch_binning(p->bound, R, INT64_MAX, kBinSymbolic, bp, p->bin_of_row, counts, offsets, cursors, p->lists, lc);
-  launches += 3;
-  // each stage: one launch per warp-table size, each reading its bin's
-  // bounds on the device
-  auto stage = [&](bool numeric) {
-    for (int b = 0; b < kNumWarpBins; ++b) {
-      const int logt = kMinLogT + b;
-      const int w = p->warps[numeric ? 1 : 0][b];
-      const size_t smem = (size_t)w * batch_table_bytes(logt, numeric);
-      const int grid = lc.sms * p->per_sm[numeric ? 1 : 0][b];
-#define SPG_BB(L)                                                                                                 \
-  case L:                                                                                                         \
-    if (numeric)                                                                                                  \
-      k_batch_bin<L, true><<<grid, w * 32, smem, lc.stream>>>(p->d_mats, p->row_mat, p->lists, offsets, p->nnz,   \
-                                                              p->nnz, p->c_col, p->c_val, ctx->d_flags);          \
-    else                                                                                                          \
-      k_batch_bin<L, false><<<grid, w * 32, smem, lc.stream>>>(p->d_mats, p->row_mat, p->lists, offsets, p->nnz, \
-                                                               nullptr, nullptr, nullptr, ctx->d_flags);          \
-    break;
-      switch (logt) {
-        SPG_BB(5) SPG_BB(6) SPG_BB(7) SPG_BB(8) SPG_BB(9) SPG_BB(10) SPG_BB(11) SPG_BB(12)
-        default: break;
-      }
-#undef SPG_BB
-      ++launches;
-    }
+  const LearnedOut lo{p->cap, p->slab_off, p->slab_col, p->slab_val, p->retry, p->lcount ? p->lcount + 1 : nullptr};
+  auto run_queue = [&](int which, bool learned) {
+    QueueArgs a{};
+    a.mats = p->d_mats;
+    a.row_mat = p->row_mat;
+    a.lists = p->lists;
+    a.bin_off = offsets;
+    a.q = queue_of(which);
+    a.tile_pref = p->tile_pref + which * (kQueueMax + 1);
+    a.bound = p->bound;
+    a.nnz = p->nnz;
+    a.gscan = p->nnz;
+    a.c_col = p->c_col;
+    a.c_val = p->c_val;
+    a.lo = lo;
+    a.counter = p->qcount + which;
+    a.flags = ctx->d_flags;
+    cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), lc.stream);
+    k_queue_prefix<<<1, 32, 0, lc.stream>>>(offsets, a.q, const_cast<int64_t*>(a.tile_pref));
+    queue_dispatch(which, learned, &a, p->grid[learned ? 1 : 0][which], queue_smem(which), lc.stream);
+    launches += 2;
   };
-  stage(false);
-  launch_binning(p->nnz, R, INT64_MAX, kBinNumeric, bp, p->bin_of_row, counts, offsets, cursors, p->lists, lc);
-  launch_excl_scan(p->nnz, R, p->nnz, p->scan_tmp, lc);
-  launches += 7;
-  stage(true);
+  auto exact_stages = [&](const int64_t* sym_key) {
+    launch_binning(sym_key, R, INT64_MAX, kBinSymbolic, p->bp_sym, p->bin_of_row, counts, offsets, cursors,
+                   p->lists, lc);
+    launches += 3;
+    run_queue(kQSymLarge, false);
+    run_queue(kQSymSmall, false);
+  };
+  if (!p->learned) {
+    exact_stages(p->bound);
+    launch_binning(p->nnz, R, INT64_MAX, kBinNumeric, p->bp_num, p->bin_of_row, counts, offsets, cursors, p->lists,
+                   lc);
+    launch_excl_scan(p->nnz, R, p->nnz, p->scan_tmp, lc);
+    launches += 7;
+    run_queue(kQNumLarge, false);
+    run_queue(kQNumMid, false);
+    run_queue(kQNumSmall, false);
+  } else {
+    cudaMemsetAsync(p->lcount, 0, 2 * sizeof(unsigned long long), lc.stream);
+    cudaMemsetAsync(p->need, 0, (size_t)std::max<int64_t>(R, 1), lc.stream);
+    launch_learned_plan_batch(p->d_mats, p->row_mat, R, ctx->mlp_w16, p->tune.predict_margin, p->tune.predict_slack,
+                              kBatchMaxBound, p->force_overflow, p->prod, p->cap, p->need, p->lcount, lc);
+    launch_binning(p->cap, R, INT64_MAX, kBinLearned, p->bp_lrn, p->bin_of_row, counts, offsets, cursors, p->lists,
+                   lc);
+    launch_excl_scan(p->cap, R, p->slab_off, p->scan_tmp, lc);
+    launches += 8;
+    run_queue(kQNumLarge, true);
+    run_queue(kQNumMid, true);
+    run_queue(kQNumSmall, true);
+    // the exact path for rows predicted beyond the tables and overflowed rows
+    launch_mark_rows(p->retry, p->lcount + 1, p->need, lc);
+    launch_mask_key(p->bound, p->need, R, p->mkey, lc);
+    launches += 2;
+    exact_stages(p->mkey);
+    launch_mask_key(p->nnz, p->need, R, p->mkey, lc);
+    launch_binning(p->mkey, R, INT64_MAX, kBinNumeric, p->bp_num, p->bin_of_row, counts, offsets, cursors, p->lists,
+                   lc);
+    launch_excl_scan(p->nnz, R, p->nnz, p->scan_tmp, lc);
+    launches += 8;
+    run_queue(kQNumLarge, false);
+    run_queue(kQNumMid, false);
+    run_queue(kQNumSmall, false);
+    k_batch_compact<<<blocks_for(R, 8), 256, 0, lc.stream>>>(p->d_mats, p->row_mat, R, p->need, p->slab_off,
+                                                            p->slab_col, p->slab_val, p->nnz, p->c_col, p->c_val);
+    ++launches;
+    cudaMemcpyAsync(p->h_lcount, p->lcount, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, lc.stream);
+  }
   k_batch_finalize<<<blocks_for(R + p->n, 256), 256, 0, lc.stream>>>(p->d_mats, p->n, p->row_mat, R, p->nnz,
                                                                      p->rp_out, p->nnz_m);
   ++launches;
@@ -299,11 +623,36 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
     // (load 0.65 measured best for the batch of 64 uneven products)
     p->tune = default_tuning();
     p->tune.max_load = 0.65f;
+    // the learned capacity already carries a margin over the prediction:
+    // fuller tables at it match the plain tables' size
+    p->tune.learned_load = 0.8f;
   }
   // every warp table size stays available on the batched path: a smaller
   // tuned maximum would send whole products to the one-by-one path
   p->tune.warp_table_max = default_tuning().warp_table_max;
-  const BinParams bp = without_block_bins(bin_params(p->tune));
+  // symbolic binning: warp tables up to 2^11 slots at load <= 2/3, the CTA
+  // table beyond; numeric: warp tables up to 2^10 slots at max_load, the CTA
+  // table beyond (both CTA tables 2^13 slots at load <= 1/2)
+  BinParams bs = without_block_bins(bin_params(p->tune));
+  bs.warp_log_max = 11;
+  bs.warp_cap = ((int64_t)1 << 11) * 2 / 3;
+  bs.block_cap = kBatchMaxBound;
+  p->bp_sym = bs;
+  BinParams bn = without_block_bins(bin_params(p->tune));
+  bn.warp_log_max = 10;
+  bn.warp_cap = (int64_t)std::floor(1024.0 * bn.max_load);
+  bn.block_min = bn.warp_cap;
+  bn.blk_small_cap = kBatchMaxBound;
+  bn.blk_large_cap = 0;
+  p->bp_num = bn;
+  // learned binning: as numeric, at the learned load factor
+  BinParams bl = bn;
+  bl.max_load = std::min(0.9f, std::max(0.1f, p->tune.learned_load > 0.f ? p->tune.learned_load : bn.max_load));
+  bl.warp_cap = (int64_t)std::floor(1024.0 * bl.max_load);
+  bl.block_min = bl.warp_cap;
+  p->bp_lrn = bl;
+  p->learned = o.algo == SPG_ALGO_LEARNED;
+  p->force_overflow = o.force_overflow;
   const LaunchCtx lc = launch_ctx(ctx);
   p->mats.resize((size_t)n);
   int64_t R = 0;
@@ -375,13 +724,13 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
   SPG_CUDA(ctx, cudaMemcpyAsync(hmax.data(), maxb, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
   SPG_CUDA(ctx, cudaMemcpyAsync(hsum.data(), sumb, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
   SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  // products whose rows exceed the warp tables go through the single path
+  // products with rows beyond the queue's tables go through the single path
   int64_t cbase = 0, rpbase = 0;
   p->c_base.assign((size_t)n, 0);
   for (int m = 0; m < n; ++m) {
     BatchMat& M = p->mats[(size_t)m];
     // the persistent kernels use 32-bit row offsets of B (nnz(B) < 2^31)
-    if ((int64_t)hmax[(size_t)m] > bp.warp_cap || !M.B.rp32) {
+    if ((int64_t)hmax[(size_t)m] > kBatchMaxBound || !M.B.rp32) {
       p->individual.push_back(m);
       // keep its rows out of the persistent stages: an empty A view
       M.A.rows = 0;
@@ -391,7 +740,7 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
     M.c_base = cbase;
     M.rp_base = rpbase;
     p->c_base[(size_t)m] = cbase;
-    if ((int64_t)hmax[(size_t)m] <= bp.warp_cap && M.B.rp32) cbase += (int64_t)hsum[(size_t)m];
+    if ((int64_t)hmax[(size_t)m] <= kBatchMaxBound && M.B.rp32) cbase += (int64_t)hsum[(size_t)m];
     rpbase += A[m].rows + 1;
   }
   if (!p->individual.empty()) {
@@ -418,46 +767,33 @@ spg_status build_plan(spg_ctx* ctx, int n, const spg_csr* A, const spg_csr* B, c
   SPG_CUDA(ctx, cudaMemcpyAsync(p->d_mats, p->mats.data(), (size_t)n * sizeof(BatchMat), cudaMemcpyHostToDevice,
                                 ctx->stream));
   SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  // CTA size, shared memory and CTAs per SM of every per-bin kernel (set
-  // before any capture): of 1..kBatchWarps warps whose tables fit
-  // kBatchCtaTableBytes, the size with the most resident warps per SM, ties
-  // to the larger CTA
-  for (int numeric = 0; numeric < 2; ++numeric) {
-    for (int b = 0; b < kNumWarpBins; ++b) {
-      const int logt = kMinLogT + b;
-      const size_t per_warp = batch_table_bytes(logt, numeric != 0);
-      const int max_w = (int)std::max<size_t>(1, std::min<size_t>(kBatchWarps, kBatchCtaTableBytes / per_warp));
-      int best_w = 1, best_ctas = 1, best = -1;
-      for (int w = 1; w <= max_w; ++w) {
-        const size_t smem = (size_t)w * per_warp;
-        int per_sm = 0;
-#define SPG_BA(L)                                                                                            \
-  case L:                                                                                                    \
-    if (numeric) {                                                                                           \
-      SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_bin<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                         (int)kBatchCtaTableBytes));                                         \
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_bin<L, true>, w * 32, smem);            \
-    } else {                                                                                                 \
-      SPG_CUDA(ctx, cudaFuncSetAttribute(k_batch_bin<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                         (int)kBatchCtaTableBytes));                                         \
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_bin<L, false>, w * 32, smem);           \
-    }                                                                                                        \
-    break;
-        switch (logt) {
-          SPG_BA(5) SPG_BA(6) SPG_BA(7) SPG_BA(8) SPG_BA(9) SPG_BA(10) SPG_BA(11) SPG_BA(12)
-          default: break;
-        }
-#undef SPG_BA
-        if (per_sm >= 1 && per_sm * w >= best) {
-          best = per_sm * w;
-          best_w = w;
-          best_ctas = per_sm;
-        }
-      }
-      p->warps[numeric][b] = best_w;
-      p->per_sm[numeric][b] = best_ctas;
+  // CTAs of every queue launch: as many as fit the SMs at once (set before
+  // any capture)
+  for (int form = 0; form < 2; ++form) {
+    for (int w = 0; w < kQueues; ++w) {
+      const size_t smem = queue_smem(w);
+      const void* k = queue_dispatch(w, form == 1, nullptr, 0, 0, nullptr);
+      SPG_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      int per_sm = 0;
+      SPG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kBlkThreads, smem));
+      p->grid[form][w] = ctx->sms * std::max(1, per_sm);
     }
   }
+  if (p->learned) {
+    // capacities, slab offsets and a slab of the bound sum (the largest
+    // capacity total), the exact-path marks and the retry list
+    SPG_TRY(dmalloc(ctx, p, &p->cap, (size_t)R + 1));
+    SPG_TRY(dmalloc(ctx, p, &p->slab_off, (size_t)R + 1));
+    SPG_TRY(dmalloc(ctx, p, &p->need, (size_t)std::max<int64_t>(R, 1)));
+    SPG_TRY(dmalloc(ctx, p, &p->mkey, (size_t)std::max<int64_t>(R, 1)));
+    SPG_TRY(dmalloc(ctx, p, &p->retry, (size_t)std::max<int64_t>(R, 1)));
+    SPG_TRY(dmalloc(ctx, p, &p->slab_col, (size_t)std::max<int64_t>(cbase, 1)));
+    SPG_TRY(dmalloc(ctx, p, &p->slab_val, (size_t)std::max<int64_t>(cbase, 1)));
+    SPG_TRY(dmalloc(ctx, p, &p->lcount, 2));
+    SPG_CUDA(ctx, cudaMallocHost(&p->h_lcount, 2 * sizeof(unsigned long long)));
+  }
+  SPG_TRY(dmalloc(ctx, p, &p->tile_pref, (size_t)kQueues * (kQueueMax + 1)));
+  SPG_TRY(dmalloc(ctx, p, &p->qcount, (size_t)kQueues));
   SPG_TRY(dmalloc(ctx, p, &p->nnz, (size_t)R + 1));
   SPG_TRY(dmalloc(ctx, p, &p->bin_of_row, (size_t)std::max<int64_t>(R, 1)));
   SPG_TRY(dmalloc(ctx, p, &p->binmeta, (size_t)(3 * kNumBins + 1)));
@@ -490,10 +826,13 @@ extern "C" spg_status spg_multiply_batched(spg_ctx* ctx, int32_t n, const spg_cs
   SPG_CUDA(ctx, cudaSetDevice(ctx->device));
   spg_opts o{};
   if (opts) o = *opts;
+  if (o.algo != SPG_ALGO_PLAIN && o.algo != SPG_ALGO_LEARNED)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "spg_multiply_batched runs the plain or learned method");
   if (report) {
     std::memset(report, 0, sizeof *report);
-    report->algo = SPG_ALGO_PLAIN;
+    report->algo = o.algo;
   }
+  if (o.algo == SPG_ALGO_LEARNED) SPG_TRY(ensure_mlp(ctx));
   auto* plan = static_cast<BatchPlan*>(ctx->batch_cache);
   if (!plan || plan->key != plan_key(ctx, n, A, B, o)) {
     free_batch_cache(ctx);
@@ -554,7 +893,6 @@ extern "C" spg_status spg_multiply_batched(spg_ctx* ctx, int32_t n, const spg_cs
   double ms_total = ms;
   for (int m : plan->individual) {
     spg_opts so = o;
-    so.algo = SPG_ALGO_PLAIN;
     so.out_location = SPG_DEVICE;
     so.out_index_bits = 64;
     spg_report r{};
@@ -570,6 +908,11 @@ extern "C" spg_status spg_multiply_batched(spg_ctx* ctx, int32_t n, const spg_cs
     for (int m : plan->batched) report->rows += A[m].rows;
     for (int m : plan->individual) report->rows += A[m].rows;
     report->rows_heavy = (int64_t)plan->individual.size();
+    if (plan->learned && plan->R > 0) {
+      // rows sized by the predictor, and those that overflowed their capacity
+      report->rows_predicted = plan->R - (int64_t)plan->h_lcount[0];
+      report->rows_overflow = (int64_t)plan->h_lcount[1];
+    }
     // products of the batched part (device sum)
     unsigned long long* d = ctx->d_counter + 3;
     cudaMemsetAsync(d, 0, 8, ctx->stream);

@@ -67,20 +67,32 @@ __device__ __forceinline__ V cta_excl_scan(V v, int64_t* wsum, V& total) {
   return r;
 }
 
-// Accumulates `row` in canonical order into the CTA table and returns its
-// number of distinct columns; LEARNED: -1 when the table filled or the row
-// has more than `cap` columns (the learned path's overflow).  Uniform over
-// the CTA.  The table is cleared here, so rows need no clean-up between them.
-template <int LOGT, bool R32, bool LEARNED>
+// Log2 of the CTA table a row of `entries` output entries uses: at load
+// <= 1/2, at least 2^8 slots (one per thread), at most 2^logt_max.
+__device__ __forceinline__ int cta_table_log(int64_t entries, int logt_max) {
+  int l = 8;
+  while (l < logt_max && ((int64_t)1 << l) < 2 * entries) ++l;
+  return l;
+}
+
+// Accumulates `row` in canonical order into the CTA table (its first 2^logt
+// slots, logt <= LOGT) and returns its number of distinct columns; LEARNED:
+// -1 when the table filled or the row has more than `cap` columns (the
+// learned path's overflow).  VALUES = false only counts the columns
+// (symbolic pass: keys only, vals and own unused).  Uniform over the CTA.
+// The table is cleared here, so rows need no clean-up between them.
+template <int LOGT, bool R32, bool LEARNED, bool VALUES = true>
 __device__ __forceinline__ int cta_accumulate_row(const DCsr& A, const DCsr& B, int32_t row, int32_t* keys,
                                                   float* vals, uint32_t* own, BlockScratch& sc, int64_t cap,
-                                                  int* flags) {
-  constexpr int T = 1 << LOGT;
+                                                  int* flags, int logt = LOGT) {
+  const int T = 1 << logt;
   const int tid = threadIdx.x, lane = lane_id(), w = tid >> 5;
   for (int s = tid; s < T; s += kBlkThreads) {
     keys[s] = kEmpty;
-    vals[s] = 0.f;
-    own[s] = 0xffffffffu;
+    if (VALUES) {
+      vals[s] = 0.f;
+      own[s] = 0xffffffffu;
+    }
   }
   if (tid == 0) {
     sc.fresh = 0;
@@ -114,7 +126,7 @@ __device__ __forceinline__ int cta_accumulate_row(const DCsr& A, const DCsr& B, 
     if (tid == 0) sc.u.st.excl[cnt] = total;
     __syncthreads();
     for (int64_t x0 = 0; x0 < total; x0 += kBlkThreads) {
-      if (step != 0 && (step & 0x7fffu) == 0) {
+      if (VALUES && step != 0 && (step & 0x7fffu) == 0) {
         // the step field of the tags wrapped: reset the order words
         for (int s = tid; s < T; s += kBlkThreads) own[s] = 0xffffffffu;
         __syncthreads();
@@ -141,14 +153,14 @@ __device__ __forceinline__ int cta_accumulate_row(const DCsr& A, const DCsr& B, 
         if (act) {
           const int64_t q = sc.u.st.bs[ent] + (pos - sc.u.st.excl[ent]);
           col = B.col[q];
-          pr = prod_rn(sc.u.st.a[ent], B.val[q]);
+          if (VALUES) pr = prod_rn(sc.u.st.a[ent], B.val[q]);
         }
       }
       int slot = -1;
       bool pending = false;
       if (act) {
         bool fresh;
-        slot = table_insert(keys, LOGT, col, kNoEpoch, fresh);
+        slot = table_insert(keys, logt, col, kNoEpoch, fresh);
         if (slot < 0) {
           sc.fail = 1;
           if (!LEARNED) raise_flag(flags, kFlagHashFull);
@@ -157,7 +169,7 @@ __device__ __forceinline__ int cta_accumulate_row(const DCsr& A, const DCsr& B, 
           my_fresh += fresh ? 1 : 0;
         }
       }
-      for (uint32_t round = 0;; ++round) {
+      for (uint32_t round = 0; VALUES; ++round) {
         const uint32_t tag = (stepcode << 17) | ((0x1ffu - round) << 8) | (uint32_t)tid;
         if (pending) atomicMin(&own[slot], tag);
         __syncthreads();
@@ -185,12 +197,14 @@ __device__ __forceinline__ int cta_accumulate_row(const DCsr& A, const DCsr& B, 
   return n;
 }
 
-// Writes the row's n entries (n <= T / 2) in column order -- the first
-// `limit` of them -- with a CTA-wide LSD radix sort; the table is consumed.
+// Writes the row's n entries (n <= 2^logt / 2, the table of
+// cta_accumulate_row) in column order -- the first `limit` of them -- with a
+// CTA-wide LSD radix sort; the table is consumed.
 template <int LOGT>
 __device__ __forceinline__ void cta_emit_row(int32_t* keys, const float* vals, uint32_t* own, BlockScratch& sc,
-                                             int n, int64_t limit, int32_t* out_col, float* out_val) {
-  constexpr int T = 1 << LOGT;
+                                             int n, int64_t limit, int32_t* out_col, float* out_val,
+                                             int logt = LOGT) {
+  const int T = 1 << logt;
   const int tid = threadIdx.x, lane = lane_id(), w = tid >> 5;
   const unsigned lt = (1u << lane) - 1u;
   int32_t* col_a = reinterpret_cast<int32_t*>(own);

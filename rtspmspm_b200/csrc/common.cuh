@@ -41,6 +41,15 @@ struct DCsr {
   const int32_t* rp32;
 };
 
+// One product of a batch: its operands and where its rows and output live.
+struct BatchMat {
+  DCsr A;
+  DCsr B;
+  int64_t row_start;  // first global row of this product
+  int64_t c_base;     // first entry of C_m in the output slab
+  int64_t rp_base;    // first entry of C_m's row pointers in the row-pointer slab
+};
+
 // Row offset type of the hot loops: int32 when R32, else int64.
 template <bool R32>
 struct RowOff {

@@ -602,9 +602,10 @@ __global__ void __launch_bounds__(kBlkThreads) k_num_block(DCsr A, DCsr B, const
     const int32_t row = rows[idx];
     const int64_t off = c_rp[row];
     const int64_t want = c_rp[row + 1] - off;
-    const int n = cta_accumulate_row<LOGT, R32, false>(A, B, row, keys, vals, own, sc, 0, flags);
+    const int lg = cta_table_log(want, LOGT);
+    const int n = cta_accumulate_row<LOGT, R32, false>(A, B, row, keys, vals, own, sc, 0, flags, lg);
     if (n != want && threadIdx.x == 0) raise_flag(flags, kFlagCountDiff);
-    cta_emit_row<LOGT>(keys, vals, own, sc, n, want, c_col + off, c_val + off);
+    cta_emit_row<LOGT>(keys, vals, own, sc, n, want, c_col + off, c_val + off, lg);
   }
 }
 
@@ -626,7 +627,9 @@ __global__ void __launch_bounds__(kBlkThreads) k_num_block_learned(DCsr A, DCsr 
   uint32_t* own = reinterpret_cast<uint32_t*>(sm_blk + 2 * T);
   for (int64_t idx = blockIdx.x; idx < nrows; idx += gridDim.x) {
     const int32_t row = rows[idx];
-    const int n = cta_accumulate_row<LOGT, R32, true>(A, B, row, keys, vals, own, sc, cap[row], flags);
+    const int64_t c = cap[row];
+    const int lg = cta_table_log(c, LOGT);
+    const int n = cta_accumulate_row<LOGT, R32, true>(A, B, row, keys, vals, own, sc, c, flags, lg);
     if (n < 0) {
       if (threadIdx.x == 0) {
         nnz_out[row] = -1;
@@ -636,7 +639,7 @@ __global__ void __launch_bounds__(kBlkThreads) k_num_block_learned(DCsr A, DCsr 
       continue;
     }
     const int64_t off = slab_off[row];
-    cta_emit_row<LOGT>(keys, vals, own, sc, n, n, slab_col + off, slab_val + off);
+    cta_emit_row<LOGT>(keys, vals, own, sc, n, n, slab_col + off, slab_val + off, lg);
     if (threadIdx.x == 0) nnz_out[row] = n;
   }
 }

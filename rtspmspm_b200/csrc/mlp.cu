@@ -319,38 +319,53 @@ __device__ __forceinline__ void capacity_of(int64_t p, int64_t cols, float o0, f
 // (row by row, the whole warp on a row), computes the tile's 128 features
 // four per lane, runs the MLP on the tile with tensor cores, and writes the
 // products, capacity and exact-path mark of every row; n_exact counts the
-// rows marked for the exact path.
-template <bool R32>
-__global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B, const __nv_bfloat16* w,
-                                                                  float margin, int slack, int64_t learn_cap,
-                                                                  int bin_gate, int force_overflow, int64_t* prod,
-                                                                  int64_t* cap,
+// rows marked for the exact path.  BATCH: rows are the global rows of a
+// batch (each row's operands from its product's descriptor, rows = R),
+// else the rows of A * B.
+template <bool R32, bool BATCH>
+__global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B, const BatchMat* mats,
+                                                                  const int32_t* row_mat, int64_t rows,
+                                                                  const __nv_bfloat16* w, float margin, int slack,
+                                                                  int64_t learn_cap, int bin_gate,
+                                                                  int force_overflow, int64_t* prod, int64_t* cap,
                                                                   uint8_t* need_exact,
                                                                   unsigned long long* n_exact) {
   __shared__ MlpSmem sm;
   __shared__ float tile[kPlanWarps][16 * kMlpIn];
   __shared__ int64_t tprod[kPlanWarps][16];
+  __shared__ int64_t tcols[kPlanWarps][16];
   __shared__ RowStats tstat[kPlanWarps][16];
   load_mlp_smem(w, sm);
   const int lane = lane_id(), wib = threadIdx.x >> 5;
-  const int64_t rows = A.rows;
   const int64_t ntiles = (rows + 15) / 16;
   for (int64_t t = blockIdx.x * (int64_t)kPlanWarps + wib; t < ntiles; t += (int64_t)gridDim.x * kPlanWarps) {
     const int64_t r0 = t * 16;
     const int nr = rows - r0 < 16 ? (int)(rows - r0) : 16;
     for (int i = 0; i < nr; ++i) {
-      const RowStats st = row_stats<R32>(A, B, r0 + i);
+      RowStats st;
+      int64_t bcols = B.cols;
+      if (BATCH) {
+        const BatchMat& M = mats[row_mat[r0 + i]];
+        st = row_stats<R32>(M.A, M.B, r0 + i - M.row_start);
+        bcols = M.B.cols;
+      } else {
+        st = row_stats<R32>(A, B, r0 + i);
+      }
       if (lane == 0) {
         tstat[wib][i] = st;
         tprod[wib][i] = st.sum;
+        tcols[wib][i] = bcols;
       }
     }
-    if (lane >= nr && lane < 16) tprod[wib][lane] = 0;
+    if (lane >= nr && lane < 16) {
+      tprod[wib][lane] = 0;
+      tcols[wib][lane] = 0;
+    }
     __syncwarp();
     // the tile's 128 features, four per lane
     for (int idx = lane; idx < 16 * kMlpIn; idx += 32) {
       const int i = idx / kMlpIn;
-      tile[wib][idx] = i < nr ? feature_of(tstat[wib][i], B.cols, idx % kMlpIn) : 0.f;
+      tile[wib][idx] = i < nr ? feature_of(tstat[wib][i], tcols[wib][i], idx % kMlpIn) : 0.f;
     }
     __syncwarp();
     float o[4];
@@ -361,7 +376,8 @@ __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B
       if (ra < rows) {
         int64_t c;
         uint8_t ex;
-        capacity_of(tprod[wib][ia], B.cols, o[0], o[1], margin, slack, learn_cap, bin_gate, force_overflow, c, ex);
+        capacity_of(tprod[wib][ia], tcols[wib][ia], o[0], o[1], margin, slack, learn_cap, bin_gate, force_overflow,
+                    c, ex);
         prod[ra] = tprod[wib][ia];
         cap[ra] = c;
         need_exact[ra] = ex;
@@ -370,7 +386,8 @@ __global__ void __launch_bounds__(kPlanWarps * 32) k_learned_plan(DCsr A, DCsr B
       if (rb < rows) {
         int64_t c;
         uint8_t ex;
-        capacity_of(tprod[wib][ib], B.cols, o[2], o[3], margin, slack, learn_cap, bin_gate, force_overflow, c, ex);
+        capacity_of(tprod[wib][ib], tcols[wib][ib], o[2], o[3], margin, slack, learn_cap, bin_gate, force_overflow,
+                    c, ex);
         prod[rb] = tprod[wib][ib];
         cap[rb] = c;
         need_exact[rb] = ex;
@@ -582,13 +599,26 @@ void launch_learned_plan(const DCsr& A, const DCsr& B, const void* w16, float ma
   const int64_t tiles = (A.rows + 15) / 16;
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((tiles + kPlanWarps - 1) / kPlanWarps, lc.sms * 8));
   if (B.rp32)
-    k_learned_plan<true><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(A, B, (const __nv_bfloat16*)w16, margin, slack,
-                                                                    learn_cap, bin_gate, force_overflow, prod, cap,
-                                                                    need_exact, n_exact);
+    k_learned_plan<true, false><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(
+        A, B, nullptr, nullptr, A.rows, (const __nv_bfloat16*)w16, margin, slack, learn_cap, bin_gate, force_overflow,
+        prod, cap, need_exact, n_exact);
   else
-    k_learned_plan<false><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(A, B, (const __nv_bfloat16*)w16, margin, slack,
-                                                                     learn_cap, bin_gate, force_overflow, prod, cap,
-                                                                     need_exact, n_exact);
+    k_learned_plan<false, false><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(
+        A, B, nullptr, nullptr, A.rows, (const __nv_bfloat16*)w16, margin, slack, learn_cap, bin_gate, force_overflow,
+        prod, cap, need_exact, n_exact);
+}
+
+void launch_learned_plan_batch(const BatchMat* mats, const int32_t* row_mat, int64_t R, const void* w16, float margin,
+                               int slack, int64_t learn_cap, int force_overflow, int64_t* prod, int64_t* cap,
+                               uint8_t* need_exact, unsigned long long* n_exact, const LaunchCtx& lc) {
+  if (R == 0) return;
+  const int64_t tiles = (R + 15) / 16;
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((tiles + kPlanWarps - 1) / kPlanWarps, lc.sms * 8));
+  const DCsr none{};
+  // every product of the batch's queue has 32-bit row offsets of B
+  k_learned_plan<true, true><<<blocks, kPlanWarps * 32, 0, lc.stream>>>(
+      none, none, mats, row_mat, R, (const __nv_bfloat16*)w16, margin, slack, learn_cap, 0, force_overflow, prod,
+      cap, need_exact, n_exact);
 }
 
 void launch_mlp_fwd_bwd(const void* w16, const float* feats, const float* targets, int64_t n, float* work,

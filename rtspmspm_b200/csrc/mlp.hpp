@@ -21,6 +21,12 @@ void launch_mlp_predict(const void* w16, const float* feats, int64_t rows, float
 void launch_learned_plan(const DCsr& A, const DCsr& B, const void* w16, float margin, int slack, int64_t learn_cap,
                          int bin_gate, int force_overflow, int64_t* prod, int64_t* cap, uint8_t* need_exact,
                          unsigned long long* n_exact, const LaunchCtx& lc);
+// The same over the R global rows of a batch (products with int32 row
+// offsets of B); no bin gate.
+struct BatchMat;
+void launch_learned_plan_batch(const BatchMat* mats, const int32_t* row_mat, int64_t R, const void* w16, float margin,
+                               int slack, int64_t learn_cap, int force_overflow, int64_t* prod, int64_t* cap,
+                               uint8_t* need_exact, unsigned long long* n_exact, const LaunchCtx& lc);
 // Forward + backward over n rows; `work` holds mlp_work_floats(n) floats;
 // grad gets the full gradient (overwritten); loss (device) the mean loss.
 void launch_mlp_fwd_bwd(const void* w16, const float* feats, const float* targets, int64_t n, float* work,

@@ -300,7 +300,8 @@ class Engine:
     def free_raw(self, c: _lib.SpgCsr) -> None:
         self.L.spg_csr_free(self.ctx, ctypes.byref(c))
 
-    def multiply_batched(self, As, Bs, use_graph=True, use_tuning=False, skip_validation=False):
+    def multiply_batched(self, As, Bs, use_graph=True, use_tuning=False, skip_validation=False, algo="plain",
+                         force_overflow=False):
         """Independent products C_i = A_i*B_i (device inputs). Returns (results, report).
 
         Results of the persistent batched path live in the engine's batch
@@ -309,7 +310,8 @@ class Engine:
         sa = (_lib.SpgCsr * n)(*[a.struct() for a in As])
         sb = (_lib.SpgCsr * n)(*[b.struct() for b in Bs])
         sc = (_lib.SpgCsr * n)()
-        o = self.opts(algo="plain", use_graph=use_graph, use_tuning=use_tuning, skip_validation=skip_validation)
+        o = self.opts(algo=algo, use_graph=use_graph, use_tuning=use_tuning, skip_validation=skip_validation,
+                      force_overflow=force_overflow)
         rep = _lib.SpgReport()
         self._check(self.L.spg_multiply_batched(self.ctx, n, sa, sb, sc, ctypes.byref(o), ctypes.byref(rep)))
         return [Result(self, sc[i]) for i in range(n)], rep.as_dict()

@@ -38,6 +38,30 @@ def test_batched_matches_oracle(use_graph):
         eng.close()
 
 
+@pytest.mark.parametrize("force_overflow", [False, True])
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batched_learned_matches_oracle(use_graph, force_overflow):
+    """Learned batch: rows sized by the predictor in one numeric pass into a
+    slab, then copied into C; with every row mispredicted (capacity 1) all
+    rows take the exact symbolic + numeric queues instead.  Two calls (the
+    second replays the graph) give the oracle's C."""
+    pairs = small_batch(16, 21) + gen.batch_uneven(count=4, seed=11, lo=2048, hi=8192, mean_lo=40.0, mean_hi=64.0)
+    eng = Engine(0)
+    try:
+        dA = [DeviceCsr.from_host(a) for a, _ in pairs]
+        dB = [DeviceCsr.from_host(b) for _, b in pairs]
+        for _ in range(2):
+            res, rep = eng.multiply_batched(dA, dB, use_graph=use_graph, algo="learned",
+                                            force_overflow=force_overflow)
+            assert rep["device_flags"] == 0
+            if force_overflow:  # every row with products overflows its capacity of 1
+                assert 0 < rep["rows_overflow"] <= rep["rows_predicted"]
+            for (A, B), C in zip(pairs, res):
+                assert_parity(C.to_host(), oracle.spgemm(A, B))
+    finally:
+        eng.close()
+
+
 def test_graph_replay_reads_new_values():
     import torch
 
@@ -58,8 +82,27 @@ def test_graph_replay_reads_new_values():
         eng.close()
 
 
+def test_batched_rows_in_the_cta_tables():
+    """Denser products: rows of 1,000-4,096 products take the CTA-wide tables
+    of the queue (symbolic and numeric), beside rows in the warp tables."""
+    pairs = gen.batch_uneven(count=8, seed=11, lo=2048, hi=8192, mean_lo=40.0, mean_hi=64.0)
+    bounds = [int(np.minimum(gen.row_products(a, b), b.cols).max()) for a, b in pairs]
+    assert max(bounds) > 1500 and max(bounds) <= 4096
+    eng = Engine(0)
+    try:
+        for graph in (False, True):
+            res, rep = eng.multiply_batched([DeviceCsr.from_host(a) for a, _ in pairs],
+                                            [DeviceCsr.from_host(b) for _, b in pairs], use_graph=graph)
+            assert rep["device_flags"] == 0 and rep["rows_heavy"] == 0
+            for (A, B), C in zip(pairs, res):
+                assert_parity(C.to_host(), oracle.spgemm(A, B))
+    finally:
+        eng.close()
+
+
 def test_batch_with_a_heavy_product_falls_back_per_product():
-    H = gen.rmat(12, 16, seed=2)  # rows beyond the warp tables
+    H = gen.rmat(13, 16, seed=2)  # rows beyond the queue's tables (more than 4,096 products, capped at the columns)
+    assert int(np.minimum(gen.row_products(H, H), H.cols).max()) > 4096
     pairs = small_batch(6, 3) + [(H, H)]
     eng = Engine(0)
     try:
@@ -82,7 +125,8 @@ def _digest(H):
             int((bits * w).sum()))
 
 
-def test_batch512_full_size_capture_then_replay():
+@pytest.mark.parametrize("algo", ["plain", "learned"])
+def test_batch512_full_size_capture_then_replay(algo):
     """The 512 uneven products (seed 1; rows, inner and column dimensions
     log-uniform on [1k, 64k], Poisson nnz/row with means U(2, 32)) through one
     batched call captured as a CUDA graph, then replayed: every product of
@@ -93,10 +137,10 @@ def test_batch512_full_size_capture_then_replay():
     try:
         dA = [DeviceCsr.from_host(a) for a, _ in pairs]
         dB = [DeviceCsr.from_host(b) for _, b in pairs]
-        res, rep = eng.multiply_batched(dA, dB, use_graph=True)
+        res, rep = eng.multiply_batched(dA, dB, use_graph=True, algo=algo)
         assert rep["device_flags"] == 0
         first = [_digest(C.to_host()) for C in res]
-        res, rep = eng.multiply_batched(dA, dB, use_graph=True)
+        res, rep = eng.multiply_batched(dA, dB, use_graph=True, algo=algo)
         assert rep["device_flags"] == 0
         assert rep["products"] == sum(int(gen.row_products(a, b).sum()) for a, b in pairs)
         tot = 0

@@ -442,15 +442,20 @@ spg_status finish_output(spg_ctx* ctx, Pipeline& P, int64_t total, const spg_opt
   return SPG_OK;
 }
 
-spg_status check_flags(spg_ctx* ctx, spg_report* rep) {
-  int f = 0;
-  SPG_TRY(read_flags(ctx, &f));
+// Status of a device flag word read back after a call's work.
+spg_status flag_status(spg_ctx* ctx, int f, spg_report* rep) {
   if (rep) rep->device_flags |= f;
   if (f & kFlagBadIndex) return fail(ctx, SPG_ERR_INVALID_ARG, "input failed validation (index out of range, "
                                                                "unsorted or duplicate columns, bad row pointers)");
   if (f & (kFlagHashFull | kFlagCountDiff)) return fail(ctx, SPG_ERR_INTERNAL, "device consistency check failed (flags %d)", f);
   if (f & kFlagWaitLimit) return fail(ctx, SPG_ERR_TIMEOUT, "a bounded device wait gave up");
   return SPG_OK;
+}
+
+spg_status check_flags(spg_ctx* ctx, spg_report* rep) {
+  int f = 0;
+  SPG_TRY(read_flags(ctx, &f));
+  return flag_status(ctx, f, rep);
 }
 
 spg_status multiply_plain(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opts& o, spg_report* rep,
@@ -523,7 +528,7 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
   launch_excl_scan(cap.as<int64_t>(), rows, slab_off.as<int64_t>(), P.scan_tmp.as<int64_t>(), lc);
   ctx->launches += 4;
   int64_t slab_total = 0;
-  constexpr int kExactSlot = 40, kRetrySlot = 41;  // h_stage words (64 in all)
+  constexpr int kExactSlot = 40;  // h_stage word (64 in all)
   SPG_TRY(stage_read(ctx, ctx->h_stage + kExactSlot, ctx->d_counter + 3, 8));
   SPG_TRY(P.fetch_offsets(slab_off.as<int64_t>() + rows, &slab_total, 1));
   const int64_t n_exact = ctx->h_stage[kExactSlot];
@@ -556,10 +561,30 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
   // (the usual case) the fix-up and the exact numeric pass are skipped
   tm.mark(SPG_STAGE_FIXUP);
   bool exact_needed = n_exact > 0;
+  int64_t total = 0;
   if (!exact_needed) {
-    SPG_TRY(stage_read(ctx, ctx->h_stage + kRetrySlot, ctx->d_counter + 2, 8));
+    // the usual case: scan the counts now and read the total, the products
+    // and the overflow count in one round trip
+    tm.mark(SPG_STAGE_SCAN);
+    launch_excl_scan(P.nnz.as<int64_t>(), rows, P.nnz.as<int64_t>(), P.scan_tmp.as<int64_t>(), lc);
+    ctx->launches += 4;
+    SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 1, P.nnz.as<int64_t>() + rows, 8));
+    SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 2, ctx->d_counter + 1, 16));
     SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    exact_needed = ctx->h_stage[kRetrySlot] > 0;
+    total = ctx->h_stage[kNumBins + 1];
+    if (rep) {
+      rep->products = ctx->h_stage[kNumBins + 2];
+      rep->rows_overflow = ctx->h_stage[kNumBins + 3];
+    }
+    if (ctx->h_stage[kNumBins + 3] > 0) {
+      // rows overflowed: undo the scan (adjacent differences give back the
+      // counts, -1 for the overflowed rows) and take the exact path
+      launch_adjacent_diff(P.nnz.as<int64_t>(), rows, key.as<int64_t>(), lc);
+      SPG_CUDA(ctx, cudaMemcpyAsync(P.nnz.get(), key.get(), (size_t)rows * 8, cudaMemcpyDeviceToDevice,
+                                    ctx->stream));
+      ++ctx->launches;
+      exact_needed = true;
+    }
   }
   // the light-row list (first `light` entries of the learned binning) is
   // kept for the compaction copy when the exact path rebins
@@ -579,18 +604,20 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
     P.bin(key.as<int64_t>(), kBinNumeric);
     ctx->launches += 1;
   }
-  tm.mark(SPG_STAGE_SCAN);
-  launch_excl_scan(P.nnz.as<int64_t>(), rows, P.nnz.as<int64_t>(), P.scan_tmp.as<int64_t>(), lc);
-  ctx->launches += 4;
-  SPG_TRY(stage_read(ctx, ctx->h_stage, P.offsets(), sizeof(int64_t) * (kNumBins + 1)));
-  SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 1, P.nnz.as<int64_t>() + rows, 8));
-  SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 2, ctx->d_counter + 1, 16));
-  SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  if (exact_needed) std::memcpy(P.h_off, ctx->h_stage, sizeof(int64_t) * (kNumBins + 1));
-  const int64_t total = ctx->h_stage[kNumBins + 1];
-  if (rep) {
-    rep->products = ctx->h_stage[kNumBins + 2];
-    rep->rows_overflow = ctx->h_stage[kNumBins + 3];
+  if (exact_needed) {
+    tm.mark(SPG_STAGE_SCAN);
+    launch_excl_scan(P.nnz.as<int64_t>(), rows, P.nnz.as<int64_t>(), P.scan_tmp.as<int64_t>(), lc);
+    ctx->launches += 4;
+    SPG_TRY(stage_read(ctx, ctx->h_stage, P.offsets(), sizeof(int64_t) * (kNumBins + 1)));
+    SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 1, P.nnz.as<int64_t>() + rows, 8));
+    SPG_TRY(stage_read(ctx, ctx->h_stage + kNumBins + 2, ctx->d_counter + 1, 16));
+    SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::memcpy(P.h_off, ctx->h_stage, sizeof(int64_t) * (kNumBins + 1));
+    total = ctx->h_stage[kNumBins + 1];
+    if (rep) {
+      rep->products = ctx->h_stage[kNumBins + 2];
+      rep->rows_overflow = ctx->h_stage[kNumBins + 3];
+    }
   }
   DevBuf c_col, c_val;
   SPG_TRY(c_col.alloc(ctx, (size_t)total * 4));
@@ -621,8 +648,15 @@ spg_status multiply_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, spg_c
   spg_status st = (o.algo == SPG_ALGO_LEARNED) ? multiply_learned(ctx, P, C, o, rep, tm)
                                                : multiply_plain(ctx, P, C, o, rep, tm);
   if (st != SPG_OK) return st;
+  // the device flags ride on the final wait: a kernel writes them into the
+  // mapped staging words, read once the end event has completed
+  constexpr int kFlagSlot = 30;
+  SPG_TRY(stage_read(ctx, ctx->h_stage + kFlagSlot, ctx->d_flags, sizeof(int)));
   tm.finish(rep);
-  return check_flags(ctx, rep);
+  int f = 0;
+  std::memcpy(&f, &ctx->h_stage[kFlagSlot], sizeof(int));
+  if (f) SPG_CUDA(ctx, cudaMemsetAsync(ctx->d_flags, 0, sizeof(int), ctx->stream));
+  return flag_status(ctx, f, rep);
 }
 
 // Value-only recompute into an existing C (structure of A*B given).

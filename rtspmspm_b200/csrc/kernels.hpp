@@ -131,6 +131,8 @@ void launch_compact_rows(const int32_t* rows, int64_t nrows, const uint8_t* need
                          const int32_t* slab_col, const float* slab_val, const int64_t* c_rp, int32_t* c_col,
                          float* c_val, const LaunchCtx& lc);
 void launch_mark_rows(const int32_t* retry, const unsigned long long* count, uint8_t* need_exact, const LaunchCtx& lc);
+// out[r] = scan[r + 1] - scan[r] (undoes an exclusive scan of rows counts).
+void launch_adjacent_diff(const int64_t* scan, int64_t rows, int64_t* out, const LaunchCtx& lc);
 void launch_mask_key(const int64_t* src, const uint8_t* mask, int64_t rows, int64_t* dst, const LaunchCtx& lc);
 
 }  // namespace spg

@@ -227,6 +227,30 @@ spg_status spg_multiply_batched(spg_ctx* ctx, int32_t n, const spg_csr* A, const
 spg_status spg_multiply_noalloc(void* stream, const spg_csr* A, const spg_csr* B, spg_csr* C,
                                 char* errbuf, int32_t errlen);
 
+/*
+ * FP64 check of a product C = A * B (C from any method, on the host or the
+ * device): every entry of C is recomputed from A and B in FP64 on the GPU
+ * (the product of two FP32 factors is exact in FP64) and compared with C's
+ * FP32 value.  Reports the max and mean |c - c64|, the max of
+ * |c - c64| / sum|a*b| (the contract's bound is 1e-5), products whose
+ * column is missing from C's row and entries of C that no product reaches.
+ * Costs a binary search in C's row per intermediate product; rows are taken
+ * in blocks of at most 2^26 entries of scratch.  The reference writes C
+ * unchecked (printResult, optixSpMSpM.cpp:452-494); no counterpart.
+ */
+typedef struct spg_check_report {
+    int64_t entries;
+    int64_t missing;            /* products whose column is absent from C's row */
+    int64_t extra;              /* entries of C that no product reaches */
+    double  max_abs_err_fp64;   /* max |c - c64| */
+    double  mean_abs_err_fp64;  /* mean |c - c64| over the reached entries */
+    double  max_rel_err;        /* max |c - c64| / sum |a*b| */
+    int32_t reserved[4];
+} spg_check_report;
+
+spg_status spg_check(spg_ctx* ctx, const spg_csr* A, const spg_csr* B, const spg_csr* C,
+                     spg_check_report* out);
+
 /* Releases a matrix allocated by the library (owner != 0); no-op otherwise. */
 spg_status spg_csr_free(spg_ctx* ctx, spg_csr* m);
 

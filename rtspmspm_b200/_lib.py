@@ -92,6 +92,15 @@ class SpgTuning(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
 
 
+class SpgCheckReport(ctypes.Structure):
+    _fields_ = [("entries", ctypes.c_int64), ("missing", ctypes.c_int64), ("extra", ctypes.c_int64),
+                ("max_abs_err_fp64", ctypes.c_double), ("mean_abs_err_fp64", ctypes.c_double),
+                ("max_rel_err", ctypes.c_double), ("reserved", ctypes.c_int32 * 4)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
+
 # (name, restype, argtypes) of every exported entry point
 _P = ctypes.POINTER
 _vp = ctypes.c_void_p
@@ -112,6 +121,7 @@ SIGNATURES = [
      [_vp, ctypes.c_int32, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgOpts), _P(SpgReport)]),
     ("spg_multiply_noalloc", ctypes.c_int32,
      [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), ctypes.c_char_p, ctypes.c_int32]),
+    ("spg_check", ctypes.c_int32, [_vp, _P(SpgCsr), _P(SpgCsr), _P(SpgCsr), _P(SpgCheckReport)]),
     ("spg_csr_free", ctypes.c_int32, [_vp, _P(SpgCsr)]),
     ("spg_csr_copy", ctypes.c_int32, [_vp, _P(SpgCsr), ctypes.c_int32, _P(SpgCsr)]),
     ("spg_csr_download", ctypes.c_int32, [_vp, _P(SpgCsr), _vp, _vp, _vp]),

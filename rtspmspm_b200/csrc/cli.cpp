@@ -14,7 +14,9 @@
 // --tune-cache tune.json, --drop-zeros (skip exact zeros like the
 // ray-tracing writer), --device N, --mlp weights.bin, --transpose-m2 (C =
 // A * B^T for rectangular inputs; the reference harness leaves these as a
-// TODO, scripts/AE_test.py:165-171).
+// TODO, scripts/AE_test.py:165-171), --check (after the timed region, C is
+// recomputed in FP64 on the GPU and its errors are printed and added to the
+// --json report).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -38,6 +40,7 @@ void usage(const char* argv0) {
                "         --mlp <filename>            Predictor weights for --algo learned\n"
                "         --drop-zeros                Skip entries whose value is exactly 0\n"
                "         --transpose-m2              Multiply by the transpose of matrix 2\n"
+               "         --check                     Report C's error against an FP64 recomputation\n"
                "         --device <n>\n"
                "         --help | -h                 Print this usage message\n",
                argv0);
@@ -53,7 +56,7 @@ int die(spg_ctx* ctx, const char* what, spg_status st) {
 
 int main(int argc, char** argv) {
   std::string m1, m2, out, log, json, tune_cache, mlp;
-  int algo = SPG_ALGO_LEARNED, device = 0, drop_zeros = 0, transpose_b = 0;
+  int algo = SPG_ALGO_LEARNED, device = 0, drop_zeros = 0, transpose_b = 0, check = 0;
   for (int i = 1; i < argc; ++i) {
     const std::string a(argv[i]);
     auto next = [&]() -> std::string {
@@ -70,6 +73,7 @@ int main(int argc, char** argv) {
     else if (a == "--mlp") mlp = next();
     else if (a == "--drop-zeros") drop_zeros = 1;
     else if (a == "--transpose-m2") transpose_b = 1;
+    else if (a == "--check") check = 1;
     else if (a == "--device") device = std::atoi(next().c_str());
     else if (a == "--algo") {
       const std::string v = next();
@@ -125,6 +129,15 @@ int main(int argc, char** argv) {
   const auto t1 = std::chrono::high_resolution_clock::now();
   if (st != SPG_OK) return die(ctx, "spg_multiply", st);
   const double ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  spg_check_report chk{};
+  if (check) {
+    if ((st = spg_check(ctx, &A, &B, &C, &chk)) != SPG_OK) return die(ctx, "spg_check", st);
+    std::fprintf(stderr,
+                 "spgemm: check vs FP64: max |err| %.3e, mean |err| %.3e, max |err|/sum|a*b| %.3e, "
+                 "%lld entries, %lld missing, %lld extra\n",
+                 chk.max_abs_err_fp64, chk.mean_abs_err_fp64, chk.max_rel_err, (long long)chk.entries,
+                 (long long)chk.missing, (long long)chk.extra);
+  }
   if (!out.empty() && (st = spg_mtx_write(ctx, out.c_str(), &C, drop_zeros)) != SPG_OK)
     return die(ctx, ("writing " + out).c_str(), st);
   if (!log.empty()) {
@@ -149,7 +162,13 @@ int main(int argc, char** argv) {
                  (long long)rep.rows_predicted, (long long)rep.rows_overflow, (long long)rep.rows_heavy);
     for (int s = 0; s < SPG_STAGE_COUNT; ++s)
       std::fprintf(f, "%s\"%s\": %.6f", s ? ", " : "", names[s], rep.ms_stage[s]);
-    std::fprintf(f, "}}\n");
+    std::fprintf(f, "}");
+    if (check)
+      std::fprintf(f, ", \"check\": {\"max_abs_err_fp64\": %.6e, \"mean_abs_err_fp64\": %.6e, "
+                      "\"max_rel_err\": %.6e, \"entries\": %lld, \"missing\": %lld, \"extra\": %lld}",
+                   chk.max_abs_err_fp64, chk.mean_abs_err_fp64, chk.max_rel_err, (long long)chk.entries,
+                   (long long)chk.missing, (long long)chk.extra);
+    std::fprintf(f, "}\n");
     std::fclose(f);
   }
   spg_csr_free(ctx, &C);

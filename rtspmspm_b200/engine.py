@@ -300,6 +300,17 @@ class Engine:
     def free_raw(self, c: _lib.SpgCsr) -> None:
         self.L.spg_csr_free(self.ctx, ctypes.byref(c))
 
+    def check(self, A, B, C) -> dict:
+        """FP64 check of C = A*B on the GPU (spg_check): max / mean |c - c64|,
+        max |c - c64| / sum|a*b|, missing and extra entries."""
+        sa, ka = self._as_struct(A, self.device)
+        sb, kb = self._as_struct(B, self.device)
+        sc, kc = (C.s, C) if isinstance(C, Result) else self._as_struct(C, self.device)
+        rep = _lib.SpgCheckReport()
+        self._check(self.L.spg_check(self.ctx, ctypes.byref(sa), ctypes.byref(sb), ctypes.byref(sc),
+                                     ctypes.byref(rep)))
+        return rep.as_dict()
+
     def multiply_batched(self, As, Bs, use_graph=True, use_tuning=False, skip_validation=False, algo="plain",
                          force_overflow=False):
         """Independent products C_i = A_i*B_i (device inputs). Returns (results, report).

@@ -46,6 +46,7 @@ int main(void) {{
   printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(spg_csr), sizeof(spg_opts), sizeof(spg_report),
          sizeof(spg_tuning), sizeof(spg_train_opts), sizeof(spg_train_report));
   printf("%zu %zu %zu\\n", offsetof(spg_csr, val), offsetof(spg_report, products), offsetof(spg_opts, skip_validation));
+  printf("%zu %zu\\n", sizeof(spg_check_report), offsetof(spg_check_report, max_rel_err));
   return 0;
 }}''')
     exe = tmp_path / "sz"
@@ -54,7 +55,8 @@ int main(void) {{
     got = [int(x) for x in out]
     want = [ctypes.sizeof(_lib.SpgCsr), ctypes.sizeof(_lib.SpgOpts), ctypes.sizeof(_lib.SpgReport),
             ctypes.sizeof(_lib.SpgTuning), ctypes.sizeof(_lib.SpgTrainOpts), ctypes.sizeof(_lib.SpgTrainReport),
-            _lib.SpgCsr.val.offset, _lib.SpgReport.products.offset, _lib.SpgOpts.skip_validation.offset]
+            _lib.SpgCsr.val.offset, _lib.SpgReport.products.offset, _lib.SpgOpts.skip_validation.offset,
+            ctypes.sizeof(_lib.SpgCheckReport), _lib.SpgCheckReport.max_rel_err.offset]
     assert got == want
 
 

@@ -34,13 +34,17 @@ def test_cli_end_to_end(tmp_path, algo):
     pa, pb, pc, pl, pj = (str(tmp_path / n) for n in ("a.mtx", "b.mtx", "c.mtx", "log.txt", "r.json"))
     write_mtx(pa, A)
     write_mtx(pb, B)
-    r = subprocess.run([CLI, "-m1", pa, "-m2", pb, "-o", pc, "-l", pl, "--algo", algo, "--json", pj],
+    r = subprocess.run([CLI, "-m1", pa, "-m2", pb, "-o", pc, "-l", pl, "--algo", algo, "--json", pj, "--check"],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     ms = float(open(pl).read())
     assert ms > 0
     rep = json.load(open(pj))
     assert rep["products"] == int(gen.row_products(A, B).sum())
+    # the per-result error report of --check (FP64 recomputation on the GPU)
+    chk = rep["check"]
+    assert chk["missing"] == 0 and chk["extra"] == 0 and chk["max_rel_err"] <= 1e-5
+    assert "check vs FP64" in r.stderr
     C = read_mtx(pc)
     R = oracle.spgemm(A, B)
     np.testing.assert_array_equal(C.row_ptr, R.row_ptr)

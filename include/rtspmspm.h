@@ -374,10 +374,12 @@ typedef struct spg_tuning {
     float   learned_load;      /* learned: table load factor at the predicted capacity */
     int32_t heavy_path;        /* rows beyond the warp tables: 0 = every column tile rescans
                                   its row of A; 1 = products staged once per tile in HBM
-                                  buckets when they fit (else as 0) */
-    int32_t block_min_nnz;     /* rows with more output entries than this (and at most 8192)
-                                  use a CTA-wide hash table; 0: those beyond a 2^10-slot
-                                  warp table at max_load; -1: off (warp tables and tiles) */
+                                  buckets when they fit (else as 0); 2 = as 0, with B-row
+                                  segments of 64+ entries in a tile copied into shared
+                                  memory by bulk copies (cp.async.bulk, mbarrier) */
+    int32_t block_min_nnz;     /* > 0: rows with more output entries than this (and at most
+                                  8192) use a CTA-wide hash table; 0 or -1 (default): off,
+                                  warp tables and heavy-row tiles only */
     int32_t reserved[2];
 } spg_tuning;
 

@@ -92,10 +92,12 @@ BinParams bin_params(const spg_tuning& t) {
   int blg = ilog2_floor(std::max(1024, std::min(32768, t.block_table_max)));
   bp.block_cap = ((int64_t)1 << blg) * 2 / 3;
   // CTA-wide numeric hash bins (tables at load <= 1/2: their key and
-  // order-word arrays are the row sort's buffers) for rows above the warp
-  // tables that stay efficient: by default those of more than 2^10 slots
-  if (t.block_min_nnz < 0) return without_block_bins(bp);
-  bp.block_min = t.block_min_nnz > 0 ? (int64_t)t.block_min_nnz : (int64_t)std::floor(1024.0 * bp.max_load);
+  // order-word arrays are the row sort's buffers) for rows of more than
+  // block_min_nnz entries, when set: measured slower than the warp tables
+  // and heavy-row tiles they replace on R-MAT scale 17 (plain 29.8 against
+  // 21.6 ms) and even on scale 20 (518 against 516 ms), so off by default
+  if (t.block_min_nnz <= 0) return without_block_bins(bp);
+  bp.block_min = (int64_t)t.block_min_nnz;
   bp.blk_small_cap = ((int64_t)1 << kBlkLogSmallT) / 2;
   bp.blk_large_cap = ((int64_t)1 << kBlkLogLargeT) / 2;
   return bp;
@@ -395,7 +397,7 @@ struct Pipeline {
                         tile_cnt.as<int32_t>(), tile_off.as<int32_t>(), ntiles, c_rp, c_col, c_val,
                         use_index ? bidx.as<int32_t>() : nullptr, use_index ? tocc.as<uint32_t>() : nullptr,
                         use_list ? work.as<int64_t>() : nullptr, use_list ? nz.as<int64_t>() + nheavy : nullptr,
-                        ctx->d_counter, ctx->d_flags, lc);
+                        ctx->d_counter, ctx->d_flags, lc, tune.heavy_path == 2);
         ctx->launches += 2;
       }
       ++ctx->launches;

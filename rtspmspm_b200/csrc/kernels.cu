@@ -922,6 +922,106 @@ __device__ __forceinline__ void tile_packed(const DCsr& B, Off bs, int len, floa
 // Units of the tile kernel handed out per atomic ticket.
 constexpr int kTicketTiles = 4;
 
+// ---- bulk-staged long segments (tuning heavy_path 2) ----------------------
+// A segment of at least kBulkMin entries inside the tile has its 16-byte
+// aligned interior copied into the warp's staging area of shared memory by
+// the bulk-copy engine (cp.async.bulk global -> shared, completion on an
+// mbarrier), kBulkPiece entries of columns and values at a time; lanes then
+// read the piece from shared memory.  The unaligned head and tail (at most
+// three entries each) take plain loads.  Entries of one B row are distinct
+// columns, so their order inside the segment does not matter.
+constexpr int kBulkPiece = 64;
+constexpr int kBulkMin = 64;
+// 32-bit words per warp: columns, values, and the mbarrier (8 bytes).
+constexpr int kBulkWarpWords = 2 * kBulkPiece + 4;
+// Iterations of a bounded mbarrier wait before the kernel gives up.
+constexpr uint32_t kBulkWaitLimit = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar));
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+  for (uint32_t it = 0; it < kBulkWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Accumulates the segment [bs, bs + len) like tile_segment, through the
+// staging area.  Returns false (kFlagWaitLimit raised) when a copy did not
+// complete within the wait limit.
+template <typename Off>
+__device__ __forceinline__ bool tile_segment_bulk(const DCsr& B, Off bs, int len, float a, int32_t c0, float* acc,
+                                                  uint32_t* bits, int32_t* st_col, float* st_val, uint32_t mbar,
+                                                  uint32_t& phase, int* flags) {
+  const int lane = lane_id();
+  const Off end = bs + (Off)len;
+  const Off h = min(end, (Off)((bs + 3) & ~(Off)3));  // first 16-byte aligned entry
+  const Off t = max(h, (Off)(end & ~(Off)3));          // end of the aligned interior
+  auto one = [&](Off q) {
+    const int32_t off = B.col[q] - c0;
+    const float pr = prod_rn(a, B.val[q]);
+    if ((uint32_t)off < (uint32_t)kTileCols) {
+      acc[off] = add_rn(acc[off], pr);
+      atomicOr(&bits[off >> 5], 1u << (off & 31));
+    } else {
+      raise_flag(flags, kFlagBadIndex);
+    }
+  };
+  // ragged head and tail: plain loads
+  if (lane < (int)(h - bs)) one(bs + (Off)lane);
+  if (lane < (int)(end - t)) one(t + (Off)lane);
+  for (Off p0 = h; p0 < t; p0 += kBulkPiece) {
+    const int n = (int)min((Off)kBulkPiece, t - p0);  // a multiple of 4 entries
+    const uint32_t bytes = (uint32_t)n * 4u;
+    __syncwarp();  // the previous piece has been read
+    if (lane == 0) {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mbar), "r"(2u * bytes)
+                   : "memory");
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+              smem_u32(st_col)),
+          "l"(B.col + p0), "r"(bytes), "r"(mbar)
+          : "memory");
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+              smem_u32(st_val)),
+          "l"(B.val + p0), "r"(bytes), "r"(mbar)
+          : "memory");
+    }
+    const bool ok = mbar_wait(mbar, phase);
+    phase ^= 1u;
+    if (!__all_sync(kFull, ok)) {
+      if (lane == 0) raise_flag(flags, kFlagWaitLimit);
+      mbar_wait(mbar, phase ^ 1u);  // once more for the copies in flight, also bounded
+      return false;
+    }
+    for (int i = lane; i < n; i += 32) {
+      const int32_t off = st_col[i] - c0;
+      const float pr = prod_rn(a, st_val[i]);
+      if ((uint32_t)off < (uint32_t)kTileCols) {
+        acc[off] = add_rn(acc[off], pr);
+        atomicOr(&bits[off >> 5], 1u << (off & 31));
+      } else {
+        raise_flag(flags, kFlagBadIndex);
+      }
+    }
+  }
+  __syncwarp();
+  return true;
+}
+
 // One warp per (heavy row, 2^kTileShift-column tile), kTicketTiles tiles
 // handed out per atomic ticket (from the list of non-empty tiles when given).  A's row is read 32 entries at a time (the next 32 loaded while the
 // current ones are processed); each entry's B row is narrowed to the tile
@@ -930,7 +1030,9 @@ constexpr int kTicketTiles = 4;
 // warp, runs of short ones packed.  Accumulator: a dense tile of floats plus
 // an occupancy bitmap, emitted in column order with coalesced stores and
 // cleared as it is read.
-template <bool R32>
+// BULK: long segments through tile_segment_bulk (kBulkWarpWords more words
+// of shared memory per warp, after the tile accumulators).
+template <bool R32, bool BULK>
 __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, const int32_t* heavy_rows, int64_t nheavy,
                                                         const int32_t* big_slot, const int32_t* tile_cnt,
                                                         const int32_t* tile_off, int ntiles, const int64_t* c_rp,
@@ -944,6 +1046,12 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
   float* acc = reinterpret_cast<float*>(sm_tile) + (size_t)wib * kTileWarpWords;
   uint32_t* bits = reinterpret_cast<uint32_t*>(acc + kTileCols);
   float* stage = reinterpret_cast<float*>(bits + kTileWords);
+  int32_t* st_col = reinterpret_cast<int32_t*>(sm_tile) + (size_t)kTileWarps * kTileWarpWords +
+                    (size_t)wib * kBulkWarpWords;
+  float* st_val = reinterpret_cast<float*>(st_col + kBulkPiece);
+  const uint32_t mbar = smem_u32(st_col + 2 * kBulkPiece);
+  uint32_t phase = 0;
+  if (BULK && lane == 0) mbar_init(mbar);
   for (int s = lane; s < kTileCols; s += 32) acc[s] = 0.f;
   for (int s = lane; s < kTileWords; s += 32) bits[s] = 0u;
   __syncwarp();
@@ -1012,7 +1120,11 @@ __global__ void __launch_bounds__(kTileWarps * 32) k_num_tile(DCsr A, DCsr B, co
           const Off sbs = __shfl_sync(kFull, bs, idx);
           const int sl = __shfl_sync(kFull, len, idx);
           const float sa = __shfl_sync(kFull, a, idx);
-          tile_segment(B, sbs, sl, sa, c0, acc, bits, flags);
+          if (BULK && sl >= kBulkMin) {
+            if (!tile_segment_bulk(B, sbs, sl, sa, c0, acc, bits, st_col, st_val, mbar, phase, flags)) return;
+          } else {
+            tile_segment(B, sbs, sl, sa, c0, acc, bits, flags);
+          }
           __syncwarp();
           ++idx;
         } else {
@@ -1475,37 +1587,46 @@ void launch_build_blocked_index(const DCsr& B, int ntiles, int32_t* bidx, const 
   k_build_blocked_index<<<grid_for(B.rows, 256, 32, lc.sms * 16), 256, 0, lc.stream>>>(B, ntiles, bidx);
 }
 
-template <bool R32>
+template <bool R32, bool BULK>
 static void num_tile_one(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy,
                          const int32_t* big_slot, const int32_t* tile_cnt, const int32_t* tile_off, int ntiles,
                          const int64_t* c_rp, int32_t* c_col, float* c_val, const int32_t* bidx,
                          const uint32_t* tocc, const int64_t* work, const int64_t* nwork,
                          unsigned long long* tile_counter, int* flags, const LaunchCtx& lc) {
-  const size_t smem = (size_t)kTileWarps * (kTileCols + kTileWords + 32) * 4;
+  const size_t smem = (size_t)kTileWarps * (kTileWarpWords + (BULK ? kBulkWarpWords : 0)) * 4;
   const int twords = (ntiles + 31) / 32;
-  cudaFuncSetAttribute(k_num_tile<R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_num_tile<R32, BULK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_tile<R32>, kTileWarps * 32, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_tile<R32, BULK>, kTileWarps * 32, smem);
   if (per_sm < 1) per_sm = 1;
   const int64_t tiles = nheavy * (int64_t)ntiles;
   const int blocks = (int)std::min<int64_t>((tiles + kTileWarps - 1) / kTileWarps, (int64_t)lc.sms * per_sm);
   cudaMemsetAsync(tile_counter, 0, sizeof(unsigned long long), lc.stream);
-  k_num_tile<R32><<<blocks, kTileWarps * 32, smem, lc.stream>>>(A, B, heavy_rows, nheavy, big_slot, tile_cnt,
-                                                                tile_off, ntiles, c_rp, c_col, c_val, bidx, tocc,
-                                                                twords, work, nwork, tile_counter, flags);
+  k_num_tile<R32, BULK><<<blocks, kTileWarps * 32, smem, lc.stream>>>(A, B, heavy_rows, nheavy, big_slot, tile_cnt,
+                                                                      tile_off, ntiles, c_rp, c_col, c_val, bidx,
+                                                                      tocc, twords, work, nwork, tile_counter,
+                                                                      flags);
 }
 
 void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
                      const int32_t* tile_cnt, const int32_t* tile_off, int ntiles, const int64_t* c_rp,
                      int32_t* c_col, float* c_val, const int32_t* bidx, const uint32_t* tocc, const int64_t* work,
-                     const int64_t* nwork, unsigned long long* tile_counter, int* flags, const LaunchCtx& lc) {
+                     const int64_t* nwork, unsigned long long* tile_counter, int* flags, const LaunchCtx& lc,
+                     bool bulk) {
   if (nheavy == 0) return;
-  if (B.rp32)
-    num_tile_one<true>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off, ntiles, c_rp, c_col, c_val, bidx,
-                       tocc, work, nwork, tile_counter, flags, lc);
-  else
-    num_tile_one<false>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off, ntiles, c_rp, c_col, c_val, bidx,
-                        tocc, work, nwork, tile_counter, flags, lc);
+  // the bulk copies need 16-byte aligned column and value arrays
+  bulk = bulk && ((reinterpret_cast<uintptr_t>(B.col) | reinterpret_cast<uintptr_t>(B.val)) & 15u) == 0;
+#define SPG_NT(R, K)                                                                                          \
+  num_tile_one<R, K>(A, B, heavy_rows, nheavy, big_slot, tile_cnt, tile_off, ntiles, c_rp, c_col, c_val, bidx, \
+                     tocc, work, nwork, tile_counter, flags, lc)
+  if (B.rp32) {
+    if (bulk) SPG_NT(true, true);
+    else SPG_NT(true, false);
+  } else {
+    if (bulk) SPG_NT(false, true);
+    else SPG_NT(false, false);
+  }
+#undef SPG_NT
 }
 
 void launch_build_tile_occupancy(int64_t rows, const int32_t* bidx, int ntiles, uint32_t* tocc, const LaunchCtx& lc) {

@@ -122,11 +122,13 @@ void launch_build_tile_occupancy(int64_t rows, const int32_t* bidx, int ntiles, 
 // bidx: blocked index of B (launch_build_blocked_index) or null (binary
 // searches); tocc: its occupancy bits or null; work/nwork: the list of
 // non-empty tiles (launch_tile_worklist) and its length on the device, or
-// null (every tile is visited)
+// null (every tile is visited); bulk: segments of 64+ entries staged into
+// shared memory by bulk copies (when B's arrays are 16-byte aligned)
 void launch_num_tile(const DCsr& A, const DCsr& B, const int32_t* heavy_rows, int64_t nheavy, const int32_t* big_slot,
                      const int32_t* tile_cnt, const int32_t* tile_off, int ntiles, const int64_t* c_rp,
                      int32_t* c_col, float* c_val, const int32_t* bidx, const uint32_t* tocc, const int64_t* work,
-                     const int64_t* nwork, unsigned long long* tile_counter, int* flags, const LaunchCtx& lc);
+                     const int64_t* nwork, unsigned long long* tile_counter, int* flags, const LaunchCtx& lc,
+                     bool bulk = false);
 void launch_compact_rows(const int32_t* rows, int64_t nrows, const uint8_t* need_exact, const int64_t* slab_off,
                          const int32_t* slab_col, const float* slab_val, const int64_t* c_rp, int32_t* c_col,
                          float* c_val, const LaunchCtx& lc);

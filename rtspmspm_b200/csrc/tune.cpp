@@ -1,14 +1,16 @@
-// Autotuner: grid search over bin thresholds (largest warp table and its
-// load factor), hash-table sizes (symbolic CTA table) and block shapes
-// (warps per CTA), timed with CUDA events on the caller's products.  No
-// reference counterpart (the reference has fixed launch parameters:
-// optixLaunch(nnzA, 1, 1), optixSpMSpM.cpp:607-608).
+// Autotuner: grid search over bin thresholds (largest warp table, its load
+// factor, and the entries above which rows take a CTA-wide table), hash-table
+// sizes and block shapes (warps per CTA), timed with CUDA events on the
+// caller's products; a batch (n > 1) searches the load factor of its queue
+// tables only, the one setting its persistent launches take.  No reference
+// counterpart (the reference has fixed launch parameters: optixLaunch(nnzA,
+// 1, 1), optixSpMSpM.cpp:607-608).
 //
 // The best setting is kept in the context and, with a cache path, stored in
 // a small JSON file keyed by (shape class, GPU name):
 //   {"entries": [{"gpu": "...", "shape": "...", "ms": t,
 //                 "warp_table_max": .., "max_load": .., "warps_per_block": ..,
-//                 "block_table_max": ..}, ...]}
+//                 "block_table_max": .., "block_min_nnz": ..}, ...]}
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -86,6 +88,7 @@ std::vector<Entry> read_cache(const char* path) {
     e.t.max_load = (float)num("max_load", e.t.max_load);
     e.t.warps_per_block = (int32_t)num("warps_per_block", e.t.warps_per_block);
     e.t.block_table_max = (int32_t)num("block_table_max", e.t.block_table_max);
+    e.t.block_min_nnz = (int32_t)num("block_min_nnz", e.t.block_min_nnz);
     out.push_back(e);
   }
   return out;
@@ -99,7 +102,8 @@ bool write_cache(const char* path, const std::vector<Entry>& es) {
     const Entry& e = es[i];
     f << "  {\"gpu\": \"" << json_escape(e.gpu) << "\", \"shape\": \"" << json_escape(e.shape) << "\", \"ms\": " << e.ms
       << ", \"warp_table_max\": " << e.t.warp_table_max << ", \"max_load\": " << e.t.max_load
-      << ", \"warps_per_block\": " << e.t.warps_per_block << ", \"block_table_max\": " << e.t.block_table_max << "}"
+      << ", \"warps_per_block\": " << e.t.warps_per_block << ", \"block_table_max\": " << e.t.block_table_max
+      << ", \"block_min_nnz\": " << e.t.block_min_nnz << "}"
       << (i + 1 < es.size() ? ",\n" : "\n");
   }
   f << "]}\n";
@@ -131,7 +135,7 @@ spg_status spg_set_tuning(spg_ctx* ctx, const spg_tuning* in) {
   if (t.predict_margin <= 0.f) t.predict_margin = d.predict_margin;
   if (t.predict_slack < 0) t.predict_slack = d.predict_slack;
   if (!(t.learned_load > 0.05f && t.learned_load < 0.95f)) t.learned_load = d.learned_load;
-  if (t.heavy_path != 0 && t.heavy_path != 1) return fail(ctx, SPG_ERR_INVALID_ARG, "heavy_path must be 0 or 1");
+  if (t.heavy_path < 0 || t.heavy_path > 2) return fail(ctx, SPG_ERR_INVALID_ARG, "heavy_path must be 0, 1 or 2");
   if (t.block_min_nnz > (1 << kBlkLogLargeT) / 2)
     return fail(ctx, SPG_ERR_INVALID_ARG, "block_min_nnz above the largest CTA table (use -1 to turn the CTA bins off)");
   ctx->tuning = t;
@@ -153,21 +157,23 @@ spg_status spg_tune(spg_ctx* ctx, int32_t n, const spg_csr* A, const spg_csr* B,
   const spg_tuning saved = ctx->tuning;
   spg_tuning win = saved;
   double win_ms = 1e30;
-  // the batched path keeps every warp table size (see batched.cu), so only a
-  // single product searches the largest table
-  const std::vector<int> tables = n > 1 ? std::vector<int>{4096} : std::vector<int>{1024, 2048, 4096};
-  const float loads[] = {0.35f, 0.5f, 0.65f};
-  const int wpbs[] = {0, 4, 8, 16};
-  const int blocks[] = {8192, 16384};
+  // a batch's queue launches take the load factor only (their table sizes
+  // and CTA shapes are fixed); a single product searches the whole grid
+  const bool batch = n > 1;
+  const std::vector<int> tables = batch ? std::vector<int>{4096} : std::vector<int>{1024, 2048, 4096};
+  const std::vector<float> loads = batch ? std::vector<float>{0.5f, 0.65f, 0.8f}
+                                         : std::vector<float>{0.35f, 0.5f, 0.65f};
+  const std::vector<int> wpbs = batch ? std::vector<int>{0} : std::vector<int>{0, 4, 8, 16};
+  const std::vector<int> block_mins = batch ? std::vector<int>{0} : std::vector<int>{0, 512};
   for (int wt : tables)
     for (float ld : loads)
       for (int wp : wpbs)
-        for (int bt : blocks) {
+        for (int bm : block_mins) {
           spg_tuning t = default_tuning();
           t.warp_table_max = wt;
           t.max_load = ld;
           t.warps_per_block = wp;
-          t.block_table_max = bt;
+          t.block_min_nnz = bm;
           t.predict_margin = saved.predict_margin;
           t.predict_slack = saved.predict_slack;
           t.learned_load = saved.learned_load;

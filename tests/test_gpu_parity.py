@@ -30,13 +30,17 @@ TUNINGS = {
     "default": {},
     # CTA hash bins off: rows beyond 32 entries go to the heavy-row tiles
     "tiny_tables": {"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5, "block_min_nnz": -1},
-    # rows beyond 166 entries in the CTA hash bins
-    "mid_tables": {"warp_table_max": 256, "block_table_max": 2048, "max_load": 0.65, "warps_per_block": 4},
+    # rows beyond 100 entries in the CTA hash bins
+    "mid_tables": {"warp_table_max": 256, "block_table_max": 2048, "max_load": 0.65, "warps_per_block": 4,
+                   "block_min_nnz": 100},
     # heavy rows through the staged per-tile buckets instead of the rescanning tile kernel
     "tiny_staged": {"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5, "heavy_path": 1,
                     "block_min_nnz": -1},
     # every row of more than 8 entries in a CTA hash bin
     "cta_bins": {"block_min_nnz": 8},
+    # heavy rows with long B-row segments staged in shared memory by bulk copies
+    "tiny_bulk": {"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5, "heavy_path": 2,
+                  "block_min_nnz": -1},
 }
 
 

@@ -392,17 +392,20 @@ def other_workload(args) -> int:
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     out = {"workload": args.workload, "steps": args.steps, "warmup": args.warmup}
+    # --profile: one method only, default settings (short runs under ncu)
+    only = [args.profile] if args.profile else ["plain", "learned"]
     if args.workload == "batch512":
+        modes = [(True, False, m) for m in only] if args.profile else None
         out.update(measure_batch(eng, gen.batch_uneven(count=args.batch_count, seed=1), args.warmup, args.steps,
-                                 flush, stream))
+                                 flush, stream, tune=not args.profile, modes=modes))
     else:
         A = gen.rmat(args.rmat_scale, 16, seed=0) if args.workload == "rmat20" else gen.erdos_renyi(4096, 4096, 8.0, 0)
-        out.update(measure_single(eng, A, ["plain", "learned"], args.warmup, args.steps, flush, stream))
-        if args.workload == "er4096":
+        out.update(measure_single(eng, A, only, args.warmup, args.steps, flush, stream))
+        if args.workload == "er4096" and not args.profile:
             dA = DeviceCsr.from_host(A)
             out["cusparse"] = measure_cusparse(eng, dA.struct(), out["products"], args.warmup, args.steps, flush,
                                                stream)
-        if args.workload == "rmat20" and not args.no_cpu:
+        if args.workload == "rmat20" and not args.no_cpu and not args.profile:
             v, info = cpu_sample(A, args.cpu_seconds)
             out["cpu_baseline"] = {"value": round(v, 4), "unit": "GFLOP/s", "cores": info["cores"], "kind": "port",
                                    "sample": sample_text(info, "the same C=A*A")}

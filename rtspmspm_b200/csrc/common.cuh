@@ -253,8 +253,12 @@ __device__ __forceinline__ float group_sum_in_lane_order(unsigned grp, float pr,
   return v;
 }
 
-// Bitonic sort of 32*E keys held in registers, E per lane; element index =
-// lane * E + e, ascending after the call.
+// Bitonic sort of 32*E keys held in registers in striped order: element
+// index = e * 32 + lane, ascending after the call.  Strides below 32 pair
+// lanes (shuffles), larger ones pair registers of one lane.  The striped
+// order makes the loads of the keys from shared memory and the stores of the
+// sorted row contiguous across lanes (stencil 96^3 learned numeric 3.54 ->
+// 3.31 ms against element index = lane * E + e).
 template <int E>
 __device__ __forceinline__ void warp_sort_keys_regs(int32_t (&key)[E]) {
   const int lane = lane_id();
@@ -263,20 +267,20 @@ __device__ __forceinline__ void warp_sort_keys_regs(int32_t (&key)[E]) {
   for (int k = 2; k <= N; k <<= 1) {
 #pragma unroll
     for (int s = k >> 1; s > 0; s >>= 1) {
-      if (s >= E) {
+      if (s < 32) {
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-          const int idx = lane * E + e;
-          const int32_t pk = __shfl_xor_sync(kFull, key[e], s / E);
+          const int idx = e * 32 + lane;
+          const int32_t pk = __shfl_xor_sync(kFull, key[e], s);
           const bool keep_small = ((idx & s) == 0) == ((idx & k) == 0);
           key[e] = keep_small ? min(pk, key[e]) : max(pk, key[e]);
         }
       } else {
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-          const int f = e ^ s;
+          const int f = e ^ (s >> 5);
           if (f > e) {
-            const int idx = lane * E + e;
+            const int idx = e * 32 + lane;
             const bool asc = (idx & k) == 0;
             const int32_t x = key[e], y = key[f];
             key[e] = asc ? min(x, y) : max(x, y);

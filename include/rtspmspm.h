@@ -380,7 +380,11 @@ typedef struct spg_tuning {
     int32_t block_min_nnz;     /* > 0: rows with more output entries than this (and at most
                                   8192) use a CTA-wide hash table; 0 or -1 (default): off,
                                   warp tables and heavy-row tiles only */
-    int32_t reserved[2];
+    int32_t esc_min_prod;      /* rows of at least this many products (0: default 128) whose
+                                  output keeps half of them or more, and that fit the warp's
+                                  table memory, are expanded, radix sorted on their columns and
+                                  folded instead of hashed; -1: off */
+    int32_t reserved;
 } spg_tuning;
 
 spg_status spg_get_tuning(spg_ctx* ctx, spg_tuning* out);

@@ -86,7 +86,8 @@ class SpgTuning(ctypes.Structure):
                 ("max_load", ctypes.c_float), ("tile_cols", ctypes.c_int32),
                 ("block_table_max", ctypes.c_int32), ("predict_margin", ctypes.c_float),
                 ("predict_slack", ctypes.c_int32), ("learned_load", ctypes.c_float),
-                ("heavy_path", ctypes.c_int32), ("block_min_nnz", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2)]
+                ("heavy_path", ctypes.c_int32), ("block_min_nnz", ctypes.c_int32), ("esc_min_prod", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}

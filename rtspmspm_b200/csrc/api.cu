@@ -339,11 +339,24 @@ struct Pipeline {
   }
 
   // Numeric pass for the rows in the current (numeric) binning, into C.
-  spg_status numeric(const int64_t* c_rp, int32_t* c_col, float* c_val, spg_report* rep) {
+  // Numeric pass; `row_prod` (the rows' products, or nullptr) lets the warp
+  // bins take expand-sort-fold rows.
+  // Expand-sort-fold settings from the tuning (esc_min_prod 0: the default
+  // threshold, -1: off).
+  EscArgs esc_args(const int64_t* row_prod) const {
+    EscArgs e;
+    e.prod = row_prod;
+    e.min_prod = tune.esc_min_prod < 0 ? 0 : (tune.esc_min_prod == 0 ? kEscMinProd : tune.esc_min_prod);
+    return e;
+  }
+
+  spg_status numeric(const int64_t* c_rp, int32_t* c_col, float* c_val, spg_report* rep,
+                     const int64_t* row_prod = nullptr) {
+    const EscArgs esc = esc_args(row_prod);
     for (int b = 0; b < kNumWarpBins; ++b) {
       if (bin_size(b) == 0) continue;
       launch_num_warp(kMinLogT + b, A.view, B.view, bin_rows(b), bin_size(b), c_rp, c_col, c_val, ctx->d_flags, lc,
-                      wpb);
+                      wpb, esc);
       ++ctx->launches;
     }
     // rows above the efficient warp tables: CTA-wide hash tables
@@ -491,7 +504,7 @@ spg_status multiply_plain(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opts&
   SPG_TRY(c_col.alloc(ctx, (size_t)total * 4));
   SPG_TRY(c_val.alloc(ctx, (size_t)total * 4));
   tm.mark(SPG_STAGE_NUMERIC);
-  SPG_TRY(P.numeric(P.nnz.as<int64_t>(), c_col.as<int32_t>(), c_val.as<float>(), rep));
+  SPG_TRY(P.numeric(P.nnz.as<int64_t>(), c_col.as<int32_t>(), c_val.as<float>(), rep, P.prod.as<int64_t>()));
   SPG_TRY(finish_output(ctx, P, total, o, c_col, c_val, C));
   if (rep) rep->nnz_c = total;
   return SPG_OK;
@@ -549,7 +562,8 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
     if (P.bin_size(b) == 0) continue;
     launch_num_warp_learned(kMinLogT + b, P.A.view, P.B.view, P.bin_rows(b), P.bin_size(b), cap.as<int64_t>(),
                             slab_off.as<int64_t>(), slab_col.as<int32_t>(), slab_val.as<float>(), P.nnz.as<int64_t>(),
-                            retry.as<int32_t>(), ctx->d_counter + 2, ctx->d_flags, lc, P.wpb);
+                            retry.as<int32_t>(), ctx->d_counter + 2, ctx->d_flags, lc, P.wpb,
+                            P.esc_args(P.prod.as<int64_t>()));
     ++ctx->launches;
   }
   for (int b : {kBinBlock, kBinDense}) {
@@ -630,7 +644,7 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
   ++ctx->launches;
   if (exact_needed) {
     tm.mark(SPG_STAGE_NUMERIC);
-    SPG_TRY(P.numeric(P.nnz.as<int64_t>(), c_col.as<int32_t>(), c_val.as<float>(), rep));
+    SPG_TRY(P.numeric(P.nnz.as<int64_t>(), c_col.as<int32_t>(), c_val.as<float>(), rep, P.prod.as<int64_t>()));
   }
   SPG_TRY(finish_output(ctx, P, total, o, c_col, c_val, C));
   if (rep) rep->nnz_c = total;

@@ -118,7 +118,7 @@ template <int LOGT, bool NUMERIC, bool LEARNED>
 __device__ __forceinline__ void warp_tile(const BatchMat* mats, const int32_t* row_mat, const int32_t* lists,
                                           int64_t first, int64_t last, int32_t* sm, int64_t* nnz,
                                           const int64_t* gscan, int32_t* c_col, float* c_val, const LearnedOut& lo,
-                                          int* flags) {
+                                          const int64_t* prod, int esc_min, int ecap, int* flags) {
   constexpr int T = 1 << LOGT;
   const int lane = lane_id();
   int32_t* keys = sm;
@@ -146,7 +146,25 @@ __device__ __forceinline__ void warp_tile(const BatchMat* mats, const int32_t* r
       const int cnt = symbolic_row<LOGT, true>(M.A, M.B, r, keys, ep, flags);
       if (lane == 0) nnz[g] = cnt;
     } else if (LEARNED) {
-      const int n = accumulate_row<LOGT, true, true>(M.A, M.B, r, keys, vals, list, ep, (int)lo.cap[g], flags);
+      const int c = (int)lo.cap[g];
+      if (esc_wanted(prod[g], c, esc_min, ecap)) {
+        // expand-sort-fold row in the warp's slot (its table wiped after)
+        const int64_t off = lo.slab_off[g];
+        const int n = esc_row<true>(M.A, M.B, r, (int)prod[g], keys, c, lo.slab_col + off, lo.slab_val + off);
+        esc_wipe(keys, T);
+        if (n >= 0) {
+          if (lane == 0) {
+            if (n > c) {
+              nnz[g] = -1;
+              lo.retry[atomicAdd(lo.retry_count, 1ull)] = (int32_t)g;
+            } else {
+              nnz[g] = n;
+            }
+          }
+          continue;
+        }
+      }
+      const int n = accumulate_row<LOGT, true, true>(M.A, M.B, r, keys, vals, list, ep, c, flags);
       if (n < 0) {
         if (lane == 0) {
           nnz[g] = -1;
@@ -159,8 +177,16 @@ __device__ __forceinline__ void warp_tile(const BatchMat* mats, const int32_t* r
       }
     } else {
       const int64_t off = M.c_base + (gscan[g] - gscan[M.row_start]);
-      numeric_row<LOGT, true, true>(M.A, M.B, r, keys, vals, list, ep, c_col + off, c_val + off,
-                                    gscan[g + 1] - gscan[g], flags);
+      const int64_t want = gscan[g + 1] - gscan[g];
+      if (esc_wanted(prod[g], want, esc_min, ecap)) {
+        const int n = esc_row<true>(M.A, M.B, r, (int)prod[g], keys, want, c_col + off, c_val + off);
+        esc_wipe(keys, T);
+        if (n >= 0) {
+          if (n != want && lane == 0) raise_flag(flags, kFlagCountDiff);
+          continue;
+        }
+      }
+      numeric_row<LOGT, true, true>(M.A, M.B, r, keys, vals, list, ep, c_col + off, c_val + off, want, flags);
     }
     if (LEARNED && ep < 0) next_row<LOGT>(keys, ep);  // plain keys: cleared after every row
     if (ep >= 0) {
@@ -198,6 +224,7 @@ __global__ void __launch_bounds__(kBlkThreads, MINB) k_batch_queue(const BatchMa
                                                                    const int64_t* bound, int64_t* nnz,
                                                                    const int64_t* gscan, int32_t* c_col,
                                                                    float* c_val, LearnedOut lo,
+                                                                   const int64_t* prod, int esc_min,
                                                                    unsigned long long* counter, int* flags) {
   extern __shared__ int32_t sm_q[];
   __shared__ unsigned long long sh_tile;
@@ -258,8 +285,10 @@ __global__ void __launch_bounds__(kBlkThreads, MINB) k_batch_queue(const BatchMa
     }
     __syncthreads();  // the CTA table's memory becomes the warps' tables
   }
-  // warp mode: each warp its own tickets and table slot
+  // warp mode: each warp its own tickets and table slot (whose words an
+  // expand-sort-fold row may use whole)
   int32_t* slot = sm_q + (size_t)wib * (NUMERIC ? numeric_words<LMAX>() : (1 << LMAX));
+  const int ecap = NUMERIC ? esc_capacity(numeric_words<LMAX>()) : 0;
   for (;;) {
     int64_t t;
     if (wib == 0 && handed >= 0) {
@@ -281,7 +310,8 @@ __global__ void __launch_bounds__(kBlkThreads, MINB) k_batch_queue(const BatchMa
 #define SPG_WT(LL)                                                                                          \
   if (L == LL && LL >= LMIN && LL <= LMAX)                                                                  \
     warp_tile<(LL >= LMIN && LL <= LMAX) ? LL : LMIN, NUMERIC, LEARNED>(mats, row_mat, lists, first, last, slot, \
-                                                                        nnz, gscan, c_col, c_val, lo, flags);
+                                                                        nnz, gscan, c_col, c_val, lo, prod,       \
+                                                                        NUMERIC ? esc_min : 0, ecap, flags);
     SPG_WT(5) SPG_WT(6) SPG_WT(7) SPG_WT(8) SPG_WT(9) SPG_WT(10) SPG_WT(11)
 #undef SPG_WT
   }
@@ -396,6 +426,8 @@ struct QueueArgs {
   int32_t* c_col;
   float* c_val;
   LearnedOut lo;
+  const int64_t* prod;
+  int esc_min;
   unsigned long long* counter;
   int* flags;
 };
@@ -405,7 +437,8 @@ const void* queue_launch(const QueueArgs* a, int grid, size_t smem, cudaStream_t
   auto k = k_batch_queue<NUMERIC, LEARNED, LMIN, LMAX, CTA, MINB>;
   if (a)
     k<<<grid, kBlkThreads, smem, st>>>(a->mats, a->row_mat, a->lists, a->bin_off, a->q, a->tile_pref, a->bound,
-                                       a->nnz, a->gscan, a->c_col, a->c_val, a->lo, a->counter, a->flags);
+                                       a->nnz, a->gscan, a->c_col, a->c_val, a->lo, a->prod, a->esc_min, a->counter,
+                                       a->flags);
   return (const void*)k;
 }
 
@@ -499,6 +532,7 @@ std::vector<uintptr_t> plan_key(spg_ctx* ctx, int n, const spg_csr* A, const spg
   k.push_back((uintptr_t)t.warps_per_block);
   k.push_back((uintptr_t)(t.learned_load * 1000.0f));
   k.push_back((uintptr_t)(o.algo == SPG_ALGO_LEARNED ? 1 + (o.force_overflow ? 1 : 0) : 0));
+  k.push_back((uintptr_t)(intptr_t)t.esc_min_prod);
   for (int m = 0; m < n; ++m) {
     for (const spg_csr* x : {&A[m], &B[m]}) {
       k.push_back((uintptr_t)x->row_ptr);
@@ -549,6 +583,8 @@ void enqueue(spg_ctx* ctx, BatchPlan* p) {
     a.c_col = p->c_col;
     a.c_val = p->c_val;
     a.lo = lo;
+    a.prod = p->prod;
+    a.esc_min = p->tune.esc_min_prod < 0 ? 0 : (p->tune.esc_min_prod == 0 ? kEscMinProd : p->tune.esc_min_prod);
     a.counter = p->qcount + which;
     a.flags = ctx->d_flags;
     cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), lc.stream);

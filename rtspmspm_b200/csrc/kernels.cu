@@ -523,10 +523,14 @@ __global__ void __launch_bounds__(kSymDenseThreads) k_sym_dense(DCsr A, DCsr B, 
 // Numeric pass: warp-level hash accumulator
 // --------------------------------------------------------------------------
 
-// Plain numeric pass: exact nnz known, writes straight into C.
+// Plain numeric pass: exact nnz known, writes straight into C.  With the
+// row products `prod` given, rows that esc_wanted() take esc_row.  56
+// registers (36 resident warps per SM at 2^9-slot tables) also with the
+// expand-sort-fold code inlined, which would take 64 unbounded.
 template <int LOGT, bool R32>
-__global__ void __launch_bounds__(512, 2) k_num_warp(DCsr A, DCsr B, const int32_t* rows, int64_t nrows,
-                                                     const int64_t* c_rp, int32_t* c_col, float* c_val, int* flags) {
+__global__ void __maxnreg__(56) k_num_warp(DCsr A, DCsr B, const int32_t* rows, int64_t nrows,
+                                                     const int64_t* c_rp, int32_t* c_col, float* c_val,
+                                                     const int64_t* prod, int esc_min, int* flags) {
   constexpr int T = 1 << LOGT;
   extern __shared__ int32_t sm_tab[];
   const int lane = lane_id();
@@ -538,22 +542,36 @@ __global__ void __launch_bounds__(512, 2) k_num_warp(DCsr A, DCsr B, const int32
   int epoch = B.cols < (1 << 24) ? 0 : kNoEpoch;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int ecap = esc_capacity(numeric_words<LOGT>());
   for (int64_t idx = gw; idx < nrows; idx += nw) {
     const int32_t row = rows[idx];
     const int64_t off = c_rp[row];
-    numeric_row<LOGT, R32>(A, B, row, keys, vals, list, epoch, c_col + off, c_val + off, c_rp[row + 1] - off, flags);
+    const int64_t want = c_rp[row + 1] - off;
+    if (prod) {
+      const int64_t p = prod[row];
+      if (esc_wanted(p, want, esc_min, ecap)) {
+        const int n = esc_row<R32>(A, B, row, (int)p, keys, want, c_col + off, c_val + off);
+        esc_wipe(keys, T);
+        if (n >= 0) {
+          if (n != want && lane == 0) raise_flag(flags, kFlagCountDiff);
+          continue;
+        }
+      }
+    }
+    numeric_row<LOGT, R32>(A, B, row, keys, vals, list, epoch, c_col + off, c_val + off, want, flags);
   }
 }
 
 // Learned single-pass numeric: table sized by the predicted capacity; the
 // row is written sorted into its slab slot.  Rows whose distinct count
 // exceeds their capacity are queued for the exact re-run (nnz_out = -1).
+// Rows that esc_wanted() (at their capacity) take esc_row.
 template <int LOGT, bool R32>
-__global__ void __launch_bounds__(512, 2) k_num_warp_learned(DCsr A, DCsr B, const int32_t* rows, int64_t nrows,
+__global__ void __maxnreg__(56) k_num_warp_learned(DCsr A, DCsr B, const int32_t* rows, int64_t nrows,
                                                              const int64_t* cap, const int64_t* slab_off,
                                                              int32_t* slab_col, float* slab_val, int64_t* nnz_out,
                                                              int32_t* retry_rows, unsigned long long* retry_count,
-                                                             int* flags) {
+                                                             const int64_t* prod, int esc_min, int* flags) {
   constexpr int T = 1 << LOGT;
   extern __shared__ int32_t sm_tab[];
   const int lane = lane_id();
@@ -565,9 +583,29 @@ __global__ void __launch_bounds__(512, 2) k_num_warp_learned(DCsr A, DCsr B, con
   int epoch = B.cols < (1 << 24) ? 0 : kNoEpoch;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int ecap = esc_capacity(numeric_words<LOGT>());
   for (int64_t idx = gw; idx < nrows; idx += nw) {
     const int32_t row = rows[idx];
     const int c = (int)cap[row];
+    if (prod) {
+      const int64_t p = prod[row];
+      if (esc_wanted(p, c, esc_min, ecap)) {
+        const int64_t off = slab_off[row];
+        const int n = esc_row<R32>(A, B, row, (int)p, keys, c, slab_col + off, slab_val + off);
+        esc_wipe(keys, T);
+        if (n >= 0) {
+          if (lane == 0) {
+            if (n > c) {
+              nnz_out[row] = -1;
+              retry_rows[atomicAdd(retry_count, 1ull)] = row;
+            } else {
+              nnz_out[row] = n;
+            }
+          }
+          continue;
+        }
+      }
+    }
     const int n = accumulate_row<LOGT, R32, true>(A, B, row, keys, vals, list, epoch, c, flags);
     if (n < 0) {
       // overflow: queue the row for the exact path
@@ -1401,7 +1439,7 @@ void launch_sym_dense(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t
 
 template <int LOGT, bool R32>
 static void num_warp_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, const int64_t* c_rp,
-                         int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb) {
+                         int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb, const EscArgs& esc) {
   cudaFuncSetAttribute(k_num_warp<LOGT, R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   static std::atomic<int> auto_w{0};
   wpb = resolve_wpb(wpb, auto_w, k_num_warp<LOGT, R32>, (size_t)numeric_words<LOGT>() * 4, wpb_for(LOGT, 8));
@@ -1410,17 +1448,19 @@ static void num_warp_one(const DCsr& A, const DCsr& B, const int32_t* rows, int6
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_num_warp<LOGT, R32>, wpb * 32, smem);
   if (per_sm < 1) per_sm = 1;
   const int blocks = grid_for(nrows, wpb, 1, lc.sms * per_sm);
-  k_num_warp<LOGT, R32><<<blocks, wpb * 32, smem, lc.stream>>>(A, B, rows, nrows, c_rp, c_col, c_val, flags);
+  k_num_warp<LOGT, R32><<<blocks, wpb * 32, smem, lc.stream>>>(A, B, rows, nrows, c_rp, c_col, c_val, esc.prod,
+                                                                esc.min_prod, flags);
 }
 
 void launch_num_warp(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
-                     const int64_t* c_rp, int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb) {
+                     const int64_t* c_rp, int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb,
+                     const EscArgs& esc) {
   if (nrows == 0) return;
   const int w = wpb <= 0 ? 0 : wpb_for(log_t, wpb);
 #define SPG_NW(L)                                                                          \
   case L:                                                                                  \
-    if (B.rp32) num_warp_one<L, true>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w); \
-    else num_warp_one<L, false>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w);       \
+    if (B.rp32) num_warp_one<L, true>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w, esc); \
+    else num_warp_one<L, false>(A, B, rows, nrows, c_rp, c_col, c_val, flags, lc, w, esc);       \
     break;
   switch (log_t) {
     SPG_NW(5) SPG_NW(6) SPG_NW(7) SPG_NW(8) SPG_NW(9) SPG_NW(10) SPG_NW(11) SPG_NW(12)
@@ -1433,7 +1473,7 @@ template <int LOGT, bool R32>
 static void num_warp_learned_one(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
                                  const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
                                  int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
-                                 const LaunchCtx& lc, int wpb) {
+                                 const LaunchCtx& lc, int wpb, const EscArgs& esc) {
   cudaFuncSetAttribute(k_num_warp_learned<LOGT, R32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   static std::atomic<int> auto_w{0};
   wpb = resolve_wpb(wpb, auto_w, k_num_warp_learned<LOGT, R32>, (size_t)numeric_words<LOGT>() * 4,
@@ -1445,23 +1485,23 @@ static void num_warp_learned_one(const DCsr& A, const DCsr& B, const int32_t* ro
   const int blocks = grid_for(nrows, wpb, 1, lc.sms * per_sm);
   k_num_warp_learned<LOGT, R32><<<blocks, wpb * 32, smem, lc.stream>>>(A, B, rows, nrows, cap, slab_off, slab_col,
                                                                         slab_val, nnz_out, retry_rows, retry_count,
-                                                                        flags);
+                                                                        esc.prod, esc.min_prod, flags);
 }
 
 void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
                              const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
                              int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
-                             const LaunchCtx& lc, int wpb) {
+                             const LaunchCtx& lc, int wpb, const EscArgs& esc) {
   if (nrows == 0) return;
   const int w = wpb <= 0 ? 0 : wpb_for(log_t, wpb);
 #define SPG_NWL(L)                                                                                             \
   case L:                                                                                                      \
     if (B.rp32)                                                                                                \
       num_warp_learned_one<L, true>(A, B, rows, nrows, cap, slab_off, slab_col, slab_val, nnz_out, retry_rows, \
-                                    retry_count, flags, lc, w);                                                \
+                                    retry_count, flags, lc, w, esc);                                                \
     else                                                                                                       \
       num_warp_learned_one<L, false>(A, B, rows, nrows, cap, slab_off, slab_col, slab_val, nnz_out,            \
-                                     retry_rows, retry_count, flags, lc, w);                                   \
+                                     retry_rows, retry_count, flags, lc, w, esc);                                   \
     break;
   switch (log_t) {
     SPG_NWL(5) SPG_NWL(6) SPG_NWL(7) SPG_NWL(8) SPG_NWL(9) SPG_NWL(10) SPG_NWL(11) SPG_NWL(12)

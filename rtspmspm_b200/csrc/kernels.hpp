@@ -84,12 +84,22 @@ void launch_sym_block(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t
 void launch_sym_dense(const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, int64_t slot_base,
                       int64_t* nnz, int32_t* big_slot, int32_t* tile_cnt, int ntiles, int* flags,
                       const LaunchCtx& lc);
+// Default smallest product count of an expand-sort-fold row.
+constexpr int kEscMinProd = 128;
+// Expand-sort-fold rows in the warp numeric kernels: the row products
+// (nullptr: off) and the smallest product count that takes the path
+// (0: off).
+struct EscArgs {
+  const int64_t* prod = nullptr;
+  int min_prod = 0;
+};
 void launch_num_warp(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
-                     const int64_t* c_rp, int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb);
+                     const int64_t* c_rp, int32_t* c_col, float* c_val, int* flags, const LaunchCtx& lc, int wpb,
+                     const EscArgs& esc = EscArgs{});
 void launch_num_warp_learned(int log_t, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows,
                              const int64_t* cap, const int64_t* slab_off, int32_t* slab_col, float* slab_val,
                              int64_t* nnz_out, int32_t* retry_rows, unsigned long long* retry_count, int* flags,
-                             const LaunchCtx& lc, int wpb);
+                             const LaunchCtx& lc, int wpb, const EscArgs& esc = EscArgs{});
 // CTA-wide hash numeric pass over the rows of bin kBinBlock (2^12-slot
 // tables) or kBinDense (2^14) of a numeric / learned binning.
 void launch_num_block(int bin, const DCsr& A, const DCsr& B, const int32_t* rows, int64_t nrows, const int64_t* c_rp,

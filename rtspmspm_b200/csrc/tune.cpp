@@ -10,7 +10,7 @@
 // a small JSON file keyed by (shape class, GPU name):
 //   {"entries": [{"gpu": "...", "shape": "...", "ms": t,
 //                 "warp_table_max": .., "max_load": .., "warps_per_block": ..,
-//                 "block_table_max": .., "block_min_nnz": ..}, ...]}
+//                 "block_table_max": .., "block_min_nnz": .., "esc_min_prod": ..}, ...]}
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -89,6 +89,7 @@ std::vector<Entry> read_cache(const char* path) {
     e.t.warps_per_block = (int32_t)num("warps_per_block", e.t.warps_per_block);
     e.t.block_table_max = (int32_t)num("block_table_max", e.t.block_table_max);
     e.t.block_min_nnz = (int32_t)num("block_min_nnz", e.t.block_min_nnz);
+    e.t.esc_min_prod = (int32_t)num("esc_min_prod", e.t.esc_min_prod);
     out.push_back(e);
   }
   return out;
@@ -103,7 +104,7 @@ bool write_cache(const char* path, const std::vector<Entry>& es) {
     f << "  {\"gpu\": \"" << json_escape(e.gpu) << "\", \"shape\": \"" << json_escape(e.shape) << "\", \"ms\": " << e.ms
       << ", \"warp_table_max\": " << e.t.warp_table_max << ", \"max_load\": " << e.t.max_load
       << ", \"warps_per_block\": " << e.t.warps_per_block << ", \"block_table_max\": " << e.t.block_table_max
-      << ", \"block_min_nnz\": " << e.t.block_min_nnz << "}"
+      << ", \"block_min_nnz\": " << e.t.block_min_nnz << ", \"esc_min_prod\": " << e.t.esc_min_prod << "}"
       << (i + 1 < es.size() ? ",\n" : "\n");
   }
   f << "]}\n";
@@ -138,6 +139,8 @@ spg_status spg_set_tuning(spg_ctx* ctx, const spg_tuning* in) {
   if (t.heavy_path < 0 || t.heavy_path > 2) return fail(ctx, SPG_ERR_INVALID_ARG, "heavy_path must be 0, 1 or 2");
   if (t.block_min_nnz > (1 << kBlkLogLargeT) / 2)
     return fail(ctx, SPG_ERR_INVALID_ARG, "block_min_nnz above the largest CTA table (use -1 to turn the CTA bins off)");
+  if (t.esc_min_prod < -1 || t.esc_min_prod > 1024)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "esc_min_prod must be -1 (off), 0 (default) or 1..1024");
   ctx->tuning = t;
   return SPG_OK;
 }

@@ -67,4 +67,8 @@ def named_pairs():
     out.append(("wide_cols", gen.erdos_renyi(2000, 2000, 6.0, 7), gen.erdos_renyi(2000, 40000, 30.0, 8)))
     out.append(("stencil12", gen.stencil27(12), None))
     out.append(("rmat12", gen.rmat(12, 16, seed=1), None))
+    # ~289 products per row, nearly all distinct: expand-sort-fold rows by default
+    out.append(("er_mid", gen.erdos_renyi(3000, 3000, 17.0, 9), None))
+    # the same rows over 2^22 columns: spans too wide for the fold's words, hashed instead
+    out.append(("esc_wide_span", gen.erdos_renyi(1500, 1500, 17.0, 10), gen.erdos_renyi(1500, 1 << 22, 17.0, 11)))
     return [(n, a, a if b is None else b) for n, a, b in out]

@@ -62,6 +62,29 @@ def test_batched_learned_matches_oracle(use_graph, force_overflow):
         eng.close()
 
 
+@pytest.mark.parametrize("algo", ["plain", "learned"])
+def test_batched_fold_rows_match_hashed_rows(algo):
+    """Rows of mostly distinct products go through the expand-sort-fold path
+    in the queue kernels (by default above 128 products, every eligible row
+    with esc_min_prod 1) or are hashed (-1): the same bits as the oracle
+    either way, over a capture and a replay each."""
+    pairs = gen.batch_uneven(count=12, seed=31, lo=256, hi=4096, mean_lo=8.0, mean_hi=28.0)
+    eng = Engine(0)
+    try:
+        dA = [DeviceCsr.from_host(a) for a, _ in pairs]
+        dB = [DeviceCsr.from_host(b) for _, b in pairs]
+        refs = [oracle.spgemm(a, b) for a, b in pairs]
+        for esc in (0, 1, -1):
+            eng.set_tuning(esc_min_prod=esc, max_load=0.8, learned_load=0.8)
+            for _ in range(2):
+                res, rep = eng.multiply_batched(dA, dB, use_graph=True, use_tuning=True, algo=algo)
+                assert rep["device_flags"] == 0
+                for R, C in zip(refs, res):
+                    assert_parity(C.to_host(), R)
+    finally:
+        eng.close()
+
+
 def test_graph_replay_reads_new_values():
     import torch
 

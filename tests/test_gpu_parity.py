@@ -41,6 +41,13 @@ TUNINGS = {
     # heavy rows with long B-row segments staged in shared memory by bulk copies
     "tiny_bulk": {"warp_table_max": 64, "block_table_max": 1024, "max_load": 0.5, "heavy_path": 2,
                   "block_min_nnz": -1},
+    # every warp-bin row that fits its warp's memory with half or more of its products distinct
+    # expanded, sorted and folded instead of hashed
+    "esc_all": {"esc_min_prod": 1},
+    # the same with learned capacities below the prediction: rows overflow out of the fold
+    "esc_tight_caps": {"esc_min_prod": 1, "predict_margin": 0.6, "predict_slack": 0},
+    # hashing only
+    "esc_off": {"esc_min_prod": -1},
 }
 
 
@@ -49,7 +56,8 @@ TUNINGS = {
 @pytest.mark.parametrize("name,A,B", PAIRS, ids=[p[0] for p in PAIRS])
 def test_parity(engine, name, A, B, algo, tuning):
     engine.set_tuning(**{**{"warp_table_max": 4096, "block_table_max": 16384, "max_load": 0.5,
-                            "warps_per_block": 8, "heavy_path": 0, "block_min_nnz": 0}, **TUNINGS[tuning]})
+                            "warps_per_block": 8, "heavy_path": 0, "block_min_nnz": 0, "esc_min_prod": 0,
+                            "predict_margin": 1.25, "predict_slack": 8}, **TUNINGS[tuning]})
     C, rep = engine.multiply(A, B, algo=algo, use_tuning=True, stage_timing=True)
     R = ref(name, A, B)
     assert_parity(C.to_host(), R)

@@ -473,21 +473,17 @@ __device__ __forceinline__ void next_row(int32_t* keys, int& epoch) {
 // ---- expand-sort-fold rows ------------------------------------------------
 // For rows whose products mostly land on distinct columns the hash table
 // costs more than it saves: the row's P products are written in canonical
-// order (columns and values), turned into words ((column - lo) << kEscIdxBits)
-// | position, radix sorted (stable, LSD) on the column bits, and folded left
+// order (columns and values), turned into words ((column - lo) << b) |
+// position (b = the bits of P - 1), radix sorted (stable, LSD) on the column
+// bits, and folded left
 // to right, each column's sum starting from 0 and adding its products in
 // canonical order, as the hash accumulators do (the same bits).  Measured on
 // Erdos-Renyi 2^18 rows of 17 entries (289 products, 286 outputs per row):
 // numeric 3.85 -> 2.31 ms; rows of 64 products stay hashed (0.55 against
 // 0.81 ms).
-constexpr int kEscIdxBits = 10;
-constexpr int kEscMax = 1 << kEscIdxBits;
-
 // Largest P that `words` 32-bit words of a warp's shared memory hold: two
 // word buffers, the values and 256 bucket counts.
-__host__ __device__ __forceinline__ int esc_capacity(int words) {
-  return (words - 256) / 3 < kEscMax ? (words - 256) / 3 : kEscMax;
-}
+__host__ __device__ __forceinline__ int esc_capacity(int words) { return (words - 256) / 3; }
 
 // True when a row of `prod` products and at least `out` output entries
 // (its exact count, or the learned capacity) takes the expand-sort-fold
@@ -497,11 +493,11 @@ __device__ __forceinline__ bool esc_wanted(int64_t prod, int64_t out, int esc_mi
   return esc_min > 0 && prod >= esc_min && prod <= cap && 2 * out >= prod;
 }
 
-// Writes the row (P products) sorted into out_col/out_val (its first `limit`
-// entries) and returns its entry count, or -1, having written nothing, when
-// its column span needs more than 31 - kEscIdxBits bits (the caller hashes
-// the row then).  `buf` holds esc_capacity(words) >= P; its contents are
-// scratch afterwards.
+// Writes the row (P >= 1 products) sorted into out_col/out_val (its first
+// `limit` entries) and returns its entry count, or -1, having written
+// nothing, when its column span and positions need more than 31 bits (the
+// caller hashes the row then).  `buf` holds esc_capacity(words) >= P; its
+// contents are scratch afterwards.
 template <bool R32>
 __device__ __forceinline__ int esc_row(const DCsr& A, const DCsr& B, int32_t row, int P, int32_t* buf, int64_t limit,
                                        int32_t* out_col, float* out_val) {
@@ -552,17 +548,19 @@ __device__ __forceinline__ int esc_row(const DCsr& A, const DCsr& B, int32_t row
   hi = (int)__reduce_max_sync(kFull, (unsigned)hi);
   const uint32_t span = P > 0 ? (uint32_t)(hi - lo) : 0u;
   const int span_bits = span ? 32 - __clz(span) : 0;
-  if (base != P || span_bits > 31 - kEscIdxBits) {
+  const int ib = P > 1 ? 32 - __clz((uint32_t)(P - 1)) : 1;  // position bits
+  const uint32_t im = (1u << ib) - 1u;
+  if (base != P || span_bits + ib > 31) {
     __syncwarp();
     return -1;
   }
   __syncwarp();
-  for (int i = lane; i < P; i += 32) wa[i] = ((wa[i] - (uint32_t)lo) << kEscIdxBits) | (uint32_t)i;
+  for (int i = lane; i < P; i += 32) wa[i] = ((wa[i] - (uint32_t)lo) << ib) | (uint32_t)i;
   __syncwarp();
   // stable LSD radix sort on the column bits, 8-bit digits
   uint32_t* src = wa;
   uint32_t* dst = wb;
-  for (int shift = kEscIdxBits; shift < kEscIdxBits + span_bits; shift += 8) {
+  for (int shift = ib; shift < ib + span_bits; shift += 8) {
     for (int b = lane; b < 256; b += 32) hist[b] = 0;
     __syncwarp();
     for (int i = lane; i < P; i += 32) atomicAdd(&hist[(src[i] >> shift) & 255u], 1);
@@ -604,15 +602,15 @@ __device__ __forceinline__ int esc_row(const DCsr& A, const DCsr& B, int32_t row
     const int i = i0 + lane;
     const bool act = i < P;
     const uint32_t w = act ? src[i] : 0u;
-    const uint32_t c = w >> kEscIdxBits;
-    const bool head = act && (i == 0 || (src[i - 1] >> kEscIdxBits) != c);
+    const uint32_t c = w >> ib;
+    const bool head = act && (i == 0 || (src[i - 1] >> ib) != c);
     const unsigned hm = __ballot_sync(kFull, head);
     if (head) {
-      float v = add_rn(0.f, vals[w & (uint32_t)(kEscMax - 1)]);
+      float v = add_rn(0.f, vals[w & im]);
       for (int j = i + 1; j < P; ++j) {
         const uint32_t wj = src[j];
-        if ((wj >> kEscIdxBits) != c) break;
-        v = add_rn(v, vals[wj & (uint32_t)(kEscMax - 1)]);
+        if ((wj >> ib) != c) break;
+        v = add_rn(v, vals[wj & im]);
       }
       const int o = count + __popc(hm & lt);
       if (o < limit) {

@@ -263,10 +263,11 @@ def timed_median(fn, k, flush, stream):
     return statistics.median(ts)
 
 
-def measure_single(eng, A, algos, warmup, steps, flush, stream, index_bits=32):
+def measure_single(eng, A, algos, warmup, steps, flush, stream, index_bits=32, use_tuning=False):
     """Per-method timings of C = A*A on device-resident A (validation off):
     median ms, GFLOP/s, and the stage breakdown, prediction and heavy-row
-    counts of one extra call with stage timing on."""
+    counts of one extra call with stage timing on (the context's tuning when
+    use_tuning, else the defaults)."""
     from rtspmspm_b200 import DeviceCsr, _lib, gen
 
     dA = DeviceCsr.from_host(A, index_bits=index_bits)
@@ -274,7 +275,7 @@ def measure_single(eng, A, algos, warmup, steps, flush, stream, index_bits=32):
     sa = dA.struct()
     out = {"rows": A.rows, "nnz_a": A.nnz, "products": products}
     for algo in algos:
-        o = eng.opts(algo=algo, skip_validation=True, stage_timing=False)
+        o = eng.opts(algo=algo, skip_validation=True, stage_timing=False, use_tuning=use_tuning)
         for _ in range(warmup):
             c = _lib.SpgCsr()
             eng.multiply_raw(sa, sa, o, c, _lib.SpgReport())
@@ -291,13 +292,15 @@ def measure_single(eng, A, algos, warmup, steps, flush, stream, index_bits=32):
         ms = timed_median(step, steps, flush, stream)
         c = _lib.SpgCsr()
         rep = _lib.SpgReport()
-        eng.multiply_raw(sa, sa, eng.opts(algo=algo, skip_validation=True, stage_timing=True), c, rep)
+        eng.multiply_raw(sa, sa, eng.opts(algo=algo, skip_validation=True, stage_timing=True, use_tuning=use_tuning),
+                         c, rep)
         eng.free_raw(c)
         r = rep.as_dict()
         out[algo] = {"ms": round(ms, 3), "gflops": round(2 * products / ms / 1e6, 2), "nnz_c": r["nnz_c"],
                      "stages_ms": {k: round(v, 3) for k, v in r["stages_ms"].items()},
                      "rows_predicted": r["rows_predicted"], "rows_overflow": r["rows_overflow"],
-                     "rows_heavy": r["rows_heavy"], "kernel_launches": holder["rep"].kernel_launches}
+                     "rows_heavy": r["rows_heavy"], "kernel_launches": holder["rep"].kernel_launches,
+                     "small_path": r["small_path"]}
         if algo == "learned":
             out[algo]["misprediction_rate"] = round(r["rows_overflow"] / max(1, r["rows_predicted"]), 6)
     if "plain" in out and "learned" in out:
@@ -422,8 +425,14 @@ def extra_workloads(args, eng, flush, stream) -> dict:
 
     out = {}
     t = time.perf_counter()
-    out["er4096"] = measure_single(eng, gen.erdos_renyi(4096, 4096, 8.0, 0), ["plain", "learned"], 3, 20, flush,
-                                   stream)
+    E = gen.erdos_renyi(4096, 4096, 8.0, 0)
+    out["er4096"] = measure_single(eng, E, ["plain", "learned"], 3, 20, flush, stream)
+    # the same product through the binned pipeline (small-product path off)
+    saved = eng.get_tuning()
+    eng.set_tuning(small_rows=-1)
+    out["er4096"]["binned"] = measure_single(eng, E, ["plain", "learned"], 3, 20, flush, stream, use_tuning=True)
+    eng.set_tuning(**saved)
+    del E
     pairs = gen.batch_uneven(count=512, seed=1)
     out["batch512"] = measure_batch(eng, pairs, 3, max(3, min(args.steps, 10)), flush, stream,
                                     modes=((True, True, "plain"), (True, False, "plain"), (True, False, "learned")))

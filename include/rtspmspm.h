@@ -117,7 +117,7 @@ typedef struct spg_report {
     int32_t algo;
     int32_t device_flags;               /* bit set of SPG_FLAG_* raised by kernels */
     int32_t kernel_launches;            /* launches issued by this call */
-    int32_t reserved;
+    int32_t small_path;                 /* 1: the call took the small-product path */
 } spg_report;
 
 #define SPG_FLAG_HASH_FULL   1  /* a hash table filled up (kernel bug guard) */
@@ -384,7 +384,10 @@ typedef struct spg_tuning {
                                   output keeps half of them or more, and that fit the warp's
                                   table memory, are expanded, radix sorted on their columns and
                                   folded instead of hashed; -1: off */
-    int32_t reserved;
+    int32_t small_rows;        /* products whose A has at most this many rows (0: default 8192),
+                                  every row of at most 2048 products, take the small-product
+                                  path in both methods (three launches, one host round trip);
+                                  -1: off */
 } spg_tuning;
 
 spg_status spg_get_tuning(spg_ctx* ctx, spg_tuning* out);

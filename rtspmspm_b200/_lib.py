@@ -57,7 +57,7 @@ class SpgReport(ctypes.Structure):
                 ("rows_predicted", ctypes.c_int64), ("rows_overflow", ctypes.c_int64),
                 ("rows_heavy", ctypes.c_int64), ("bin_rows", ctypes.c_int64 * SPG_NUM_BINS),
                 ("algo", ctypes.c_int32), ("device_flags", ctypes.c_int32),
-                ("kernel_launches", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("kernel_launches", ctypes.c_int32), ("small_path", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {
@@ -67,6 +67,7 @@ class SpgReport(ctypes.Structure):
             "rows_predicted": self.rows_predicted, "rows_overflow": self.rows_overflow,
             "rows_heavy": self.rows_heavy, "bin_rows": list(self.bin_rows),
             "device_flags": self.device_flags, "kernel_launches": self.kernel_launches,
+            "small_path": self.small_path,
         }
 
 
@@ -87,7 +88,7 @@ class SpgTuning(ctypes.Structure):
                 ("block_table_max", ctypes.c_int32), ("predict_margin", ctypes.c_float),
                 ("predict_slack", ctypes.c_int32), ("learned_load", ctypes.c_float),
                 ("heavy_path", ctypes.c_int32), ("block_min_nnz", ctypes.c_int32), ("esc_min_prod", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("small_rows", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}

@@ -651,6 +651,84 @@ spg_status multiply_learned(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opt
   return SPG_OK;
 }
 
+// Rows of A up to which a call takes the small-product path (0: off).
+int64_t small_rows_limit(const spg_tuning& t) {
+  if (t.small_rows < 0) return 0;
+  return t.small_rows == 0 ? kSmallDefaultRows : std::min<int64_t>(t.small_rows, kSmallMaxRows);
+}
+
+// Small products in both methods: exact counts and products in one launch,
+// one CTA scanning them into C's row pointers, one round trip for the
+// total, and one numeric launch over every row with a table sized for the
+// largest row.  The binned pipeline spends about two dozen launches and
+// three round trips on a product of this size, which is all its time
+// (Erdos-Renyi 4096 rows of Poisson(8): 0.26 ms); the prediction cannot pay
+// for itself here either.  *taken stays false, with nothing written to C,
+// when a row has more than 2^kSmallLogT products or needs a larger table
+// than the tuning allows; the caller then runs the binned pipeline.
+spg_status multiply_small(spg_ctx* ctx, Pipeline& P, spg_csr* C, const spg_opts& o, spg_report* rep, StageTimer& tm,
+                          bool* taken) {
+  *taken = false;
+  const LaunchCtx lc = P.lc;
+  const int64_t rows = P.rows;
+  const int bits = o.out_index_bits;
+  if (bits != 0 && bits != 32 && bits != 64) return fail(ctx, SPG_ERR_INVALID_ARG, "out_index_bits must be 0, 32 or 64");
+  DevBuf rp32;
+  if (bits != 64) SPG_TRY(rp32.alloc(ctx, (size_t)(rows + 1) * 4));
+  tm.mark(SPG_STAGE_SYMBOLIC);
+  // d_counter[6]: the counting launch's stop word (zero between calls)
+  launch_small_count(P.A.view, P.B.view, P.prod.as<int64_t>(), P.nnz.as<int64_t>(), ctx->d_counter + 6, ctx->d_flags,
+                     lc);
+  tm.mark(SPG_STAGE_SCAN);
+  constexpr int kSmallSlot = 48;  // h_stage words 48..51
+  launch_small_scan(P.nnz.as<int64_t>(), P.prod.as<int64_t>(), rows, bits != 64 ? rp32.as<int32_t>() : nullptr,
+                    P.lists.as<int32_t>(), ctx->d_counter + 6, ctx->h_stage_dev + kSmallSlot, lc);
+  ctx->launches += 2;
+  SPG_CUDA(ctx, cudaGetLastError());
+  SPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const int64_t total = ctx->h_stage[kSmallSlot], products = ctx->h_stage[kSmallSlot + 1];
+  const int64_t max_cnt = ctx->h_stage[kSmallSlot + 2], too_large = ctx->h_stage[kSmallSlot + 3];
+  // the numeric table: the smallest that holds the largest row at the load factor
+  int log_t = kMinLogT;
+  while (log_t < kMaxLogT && (double)max_cnt > (double)P.tune.max_load * (double)(1 << log_t)) ++log_t;
+  if (too_large > 0 || max_cnt > (1 << log_t) || (1 << log_t) > std::max(32, P.tune.warp_table_max)) {
+    // the binned pipeline takes the call, from zeroed counts
+    SPG_CUDA(ctx, cudaMemsetAsync(P.nnz.get(), 0, (size_t)(rows + 1) * 8, ctx->stream));
+    return SPG_OK;
+  }
+  if (bits == 32 && total >= INT32_MAX)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "nnz(C)=%lld does not fit int32 row pointers", (long long)total);
+  DevBuf c_col, c_val;
+  SPG_TRY(c_col.alloc(ctx, (size_t)total * 4));
+  SPG_TRY(c_val.alloc(ctx, (size_t)total * 4));
+  tm.mark(SPG_STAGE_NUMERIC);
+  if (total > 0) {
+    launch_num_warp(log_t, P.A.view, P.B.view, P.lists.as<int32_t>(), rows, P.nnz.as<int64_t>(), c_col.as<int32_t>(),
+                    c_val.as<float>(), ctx->d_flags, lc, P.wpb, P.esc_args(P.prod.as<int64_t>()));
+    ++ctx->launches;
+  }
+  const bool narrow = bits != 64 && total < INT32_MAX;
+  std::memset(C, 0, sizeof *C);
+  C->rows = rows;
+  C->cols = P.cols;
+  C->nnz = total;
+  C->capacity = total;
+  C->index_bits = narrow ? 32 : 64;
+  C->location = SPG_DEVICE;
+  C->row_ptr = narrow ? rp32.release() : P.nnz.release();
+  C->col_idx = static_cast<int32_t*>(c_col.release());
+  C->val = static_cast<float*>(c_val.release());
+  C->owner = 1;
+  if (rep) {
+    rep->products = products;
+    rep->nnz_c = total;
+    rep->small_path = 1;
+    rep->bin_rows[log_t - kMinLogT] += rows;
+  }
+  *taken = true;
+  return SPG_OK;
+}
+
 }  // namespace
 
 namespace spg {
@@ -661,9 +739,14 @@ spg_status multiply_device(spg_ctx* ctx, const DevMat& A, const DevMat& B, spg_c
   const spg_tuning t = o.use_tuning ? ctx->tuning : default_tuning();
   Pipeline P(ctx, A, B, t);
   SPG_TRY(P.init());
-  spg_status st = (o.algo == SPG_ALGO_LEARNED) ? multiply_learned(ctx, P, C, o, rep, tm)
-                                               : multiply_plain(ctx, P, C, o, rep, tm);
-  if (st != SPG_OK) return st;
+  bool small = false;
+  if (P.rows > 0 && P.rows <= small_rows_limit(t) && !o.force_overflow)
+    SPG_TRY(multiply_small(ctx, P, C, o, rep, tm, &small));
+  if (!small) {
+    spg_status st = (o.algo == SPG_ALGO_LEARNED) ? multiply_learned(ctx, P, C, o, rep, tm)
+                                                 : multiply_plain(ctx, P, C, o, rep, tm);
+    if (st != SPG_OK) return st;
+  }
   // the device flags ride on the final wait: a kernel writes them into the
   // mapped staging words, read once the end event has completed
   constexpr int kFlagSlot = 30;

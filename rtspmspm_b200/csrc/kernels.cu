@@ -1240,6 +1240,122 @@ __global__ void k_mask_key(const int64_t* src, const uint8_t* mask, int64_t rows
 }
 
 // --------------------------------------------------------------------------
+// Small products: a counting launch, a one-CTA scan and one numeric launch
+// --------------------------------------------------------------------------
+
+// Warp per row of a small product: the row's products (prod[row]) and, for
+// rows of at most 2^kSmallLogT products, its exact output count from an
+// epoch-tagged key table of 2^kSmallLogT slots (nnz[row]).  A row with more
+// products gets nnz[row] = -1, which sends the call to the binned pipeline,
+// and sets *stop, after which rows not yet counted are marked -1 too (the
+// counts are of no use then); k_small_scan clears *stop.
+template <bool R32>
+__global__ void __launch_bounds__(kSmallCountWarps * 32) k_small_count(DCsr A, DCsr B, int64_t* prod, int64_t* nnz,
+                                                                       unsigned long long* stop, int* flags) {
+  using Off = typename RowOff<R32>::T;
+  constexpr int T = 1 << kSmallLogT;
+  extern __shared__ int32_t sm_keys[];
+  const int lane = lane_id();
+  int32_t* keys = sm_keys + (threadIdx.x >> 5) * T;
+  for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
+  __syncwarp();
+  int epoch = B.cols < (1 << 24) ? 0 : kNoEpoch;
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = gw; row < A.rows; row += nw) {
+    const unsigned long long stopped = *reinterpret_cast<volatile unsigned long long*>(stop);
+    const int64_t s = A.rp[row], e = A.rp[row + 1];
+    int64_t p = 0;
+    for (int64_t q = s + lane; q < e; q += 32) {
+      const int32_t k = A.col[q];
+      p += (int64_t)(RowOff<R32>::at(B, k + 1) - RowOff<R32>::at(B, k));
+    }
+    p = warp_sum(p);
+    int64_t cnt = -1;
+    if (p == 0) {
+      cnt = 0;
+    } else if (p <= T && !stopped) {
+      cnt = symbolic_row<kSmallLogT, R32>(A, B, (int32_t)row, keys, epoch, flags);
+      if (epoch >= 0) next_row<kSmallLogT>(keys, epoch);
+    } else if (p > T && lane == 0) {
+      *reinterpret_cast<volatile unsigned long long*>(stop) = 1ull;
+    }
+    if (lane == 0) {
+      prod[row] = p;
+      nnz[row] = cnt;
+    }
+  }
+}
+
+// One CTA over the counts of a small product (rows <= kSmallMaxRows): the
+// exclusive scan into C's int64 row pointers in place (nnz[rows] = the
+// total) and, when rp32 is given and the total fits, into int32 row
+// pointers; the identity row list of the numeric launch; and, into the
+// mapped host words out[0..3], the total, the products, the largest count
+// and the number of rows too large to count (any of them sends the call to
+// the binned pipeline).  Thread t owns rows [t * per, (t + 1) * per).
+__global__ void __launch_bounds__(kSmallScanThreads) k_small_scan(int64_t* nnz, const int64_t* prod, int64_t rows,
+                                                                  int32_t* rp32, int32_t* row_list,
+                                                                  unsigned long long* stop, volatile int64_t* out) {
+  constexpr int kW = kSmallScanThreads / 32;
+  __shared__ int64_t wsum[kW], wprod[kW], wmax[kW], wbig[kW];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int64_t per = (rows + kSmallScanThreads - 1) / kSmallScanThreads;
+  const int64_t r0 = min(rows, (int64_t)t * per), r1 = min(rows, r0 + per);
+  int64_t sum = 0, psum = 0, mx = 0, big = 0;
+  for (int64_t r = r0; r < r1; ++r) {
+    const int64_t c = nnz[r];
+    if (c < 0) {
+      ++big;
+    } else {
+      sum += c;
+      mx = max(mx, c);
+    }
+    psum += prod[r];
+    row_list[r] = (int32_t)r;
+  }
+  const int64_t incl = warp_incl_scan(sum);
+  const int64_t ps = warp_sum(psum), mm = warp_max(mx), bb = warp_sum(big);
+  if (lane == 31) wsum[w] = incl;
+  if (lane == 0) {
+    wprod[w] = ps;
+    wmax[w] = mm;
+    wbig[w] = bb;
+  }
+  __syncthreads();
+  int64_t wexcl = 0, total = 0;
+  {
+    const int64_t v = lane < kW ? wsum[lane] : 0;
+    const int64_t vi = warp_incl_scan(v);
+    wexcl = __shfl_sync(kFull, vi - v, w);
+    total = __shfl_sync(kFull, vi, 31);
+  }
+  int64_t run = wexcl + incl - sum;
+  const bool narrow = rp32 != nullptr && total < INT32_MAX;
+  for (int64_t r = r0; r < r1; ++r) {
+    const int64_t c = nnz[r];
+    nnz[r] = run;
+    if (narrow) rp32[r] = (int32_t)run;
+    run += c < 0 ? 0 : c;
+  }
+  if (t == 0) {
+    nnz[rows] = total;
+    if (narrow) rp32[rows] = (int32_t)total;
+    int64_t p = 0, m = 0, b = 0;
+    for (int i = 0; i < kW; ++i) {
+      p += wprod[i];
+      m = max(m, wmax[i]);
+      b += wbig[i];
+    }
+    out[0] = total;
+    out[1] = p;
+    out[2] = m;
+    out[3] = b;
+    *stop = 0ull;
+  }
+}
+
+// --------------------------------------------------------------------------
 // Host launchers
 // --------------------------------------------------------------------------
 
@@ -1266,6 +1382,23 @@ void launch_validate(const DCsr& M, int64_t nnz, int* flags, const LaunchCtx& lc
 void launch_row_products(const DCsr& A, const DCsr& B, int64_t* prod, const LaunchCtx& lc) {
   if (A.rows == 0) return;
   k_row_products<<<grid_for(A.rows, 256, 32, lc.sms * 16), 256, 0, lc.stream>>>(A, B, prod);
+}
+
+void launch_small_count(const DCsr& A, const DCsr& B, int64_t* prod, int64_t* nnz, unsigned long long* stop,
+                        int* flags, const LaunchCtx& lc) {
+  if (A.rows == 0) return;
+  const size_t smem = (size_t)kSmallCountWarps * (1u << kSmallLogT) * 4;
+  int per_sm = 0;
+  if (B.rp32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_small_count<true>, kSmallCountWarps * 32, smem);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_small_count<false>, kSmallCountWarps * 32, smem);
+  const int blocks = grid_for(A.rows, kSmallCountWarps, 1, lc.sms * (per_sm < 1 ? 1 : per_sm));
+  if (B.rp32) k_small_count<true><<<blocks, kSmallCountWarps * 32, smem, lc.stream>>>(A, B, prod, nnz, stop, flags);
+  else k_small_count<false><<<blocks, kSmallCountWarps * 32, smem, lc.stream>>>(A, B, prod, nnz, stop, flags);
+}
+
+void launch_small_scan(int64_t* nnz, const int64_t* prod, int64_t rows, int32_t* rp32, int32_t* row_list,
+                       unsigned long long* stop, int64_t* out, const LaunchCtx& lc) {
+  k_small_scan<<<1, kSmallScanThreads, 0, lc.stream>>>(nnz, prod, rows, rp32, row_list, stop, out);
 }
 
 void launch_sum(const int64_t* v, int64_t n, unsigned long long* out, const LaunchCtx& lc) {

@@ -69,6 +69,26 @@ void launch_widen_rp(const int32_t* in, int64_t n, int64_t* out, const LaunchCtx
 void launch_narrow_rp(const int64_t* in, int64_t n, int32_t* out, const LaunchCtx& lc);
 void launch_validate(const DCsr& M, int64_t nnz, int* flags, const LaunchCtx& lc);
 void launch_row_products(const DCsr& A, const DCsr& B, int64_t* prod, const LaunchCtx& lc);
+
+// Small products (at most kSmallMaxRows rows of A, every row of at most
+// 2^kSmallLogT products): products and exact counts per row in one launch
+// (nnz[row] = -1 for a row of more products), then one CTA scans the counts
+// into C's row pointers (int64 in place, int32 into rp32 when given and the
+// total fits), writes the identity row list and puts the total, the
+// products, the largest count and the too-large rows into out[0..3]
+// (mapped host words).
+constexpr int kSmallLogT = 11;
+constexpr int kSmallCountWarps = 4;
+constexpr int kSmallScanThreads = 1024;
+constexpr int64_t kSmallMaxRows = 65536;
+constexpr int kSmallDefaultRows = 8192;
+// `stop` (one device word, zero between calls): set by the counting launch
+// at its first too-large row so that the remaining rows skip their counts;
+// the scan clears it.
+void launch_small_count(const DCsr& A, const DCsr& B, int64_t* prod, int64_t* nnz, unsigned long long* stop,
+                        int* flags, const LaunchCtx& lc);
+void launch_small_scan(int64_t* nnz, const int64_t* prod, int64_t rows, int32_t* rp32, int32_t* row_list,
+                       unsigned long long* stop, int64_t* out, const LaunchCtx& lc);
 void launch_sum(const int64_t* v, int64_t n, unsigned long long* out, const LaunchCtx& lc);
 void launch_binning(const int64_t* key, int64_t rows, int64_t cols, int mode, const BinParams& bp,
                     uint8_t* bin_of_row, int64_t* counts, int64_t* offsets, int64_t* cursors, int32_t* lists,

@@ -141,6 +141,8 @@ spg_status spg_set_tuning(spg_ctx* ctx, const spg_tuning* in) {
     return fail(ctx, SPG_ERR_INVALID_ARG, "block_min_nnz above the largest CTA table (use -1 to turn the CTA bins off)");
   if (t.esc_min_prod < -1 || t.esc_min_prod > 1024)
     return fail(ctx, SPG_ERR_INVALID_ARG, "esc_min_prod must be -1 (off), 0 (default) or 1..1024");
+  if (t.small_rows < -1 || t.small_rows > kSmallMaxRows)
+    return fail(ctx, SPG_ERR_INVALID_ARG, "small_rows must be -1 (off), 0 (default) or 1..65536");
   ctx->tuning = t;
   return SPG_OK;
 }

@@ -48,6 +48,8 @@ TUNINGS = {
     "esc_tight_caps": {"esc_min_prod": 1, "predict_margin": 0.6, "predict_slack": 0},
     # hashing only
     "esc_off": {"esc_min_prod": -1},
+    # the small-product path for every case it takes (heavy_row and rmat12 fall back to the bins)
+    "small": {"small_rows": 65536},
 }
 
 
@@ -57,7 +59,7 @@ TUNINGS = {
 def test_parity(engine, name, A, B, algo, tuning):
     engine.set_tuning(**{**{"warp_table_max": 4096, "block_table_max": 16384, "max_load": 0.5,
                             "warps_per_block": 8, "heavy_path": 0, "block_min_nnz": 0, "esc_min_prod": 0,
-                            "predict_margin": 1.25, "predict_slack": 8}, **TUNINGS[tuning]})
+                            "predict_margin": 1.25, "predict_slack": 8, "small_rows": -1}, **TUNINGS[tuning]})
     C, rep = engine.multiply(A, B, algo=algo, use_tuning=True, stage_timing=True)
     R = ref(name, A, B)
     assert_parity(C.to_host(), R)
@@ -78,6 +80,40 @@ def test_cta_sizes(engine, algo, wpb):
     for bad in (-1, 17):
         with pytest.raises(SpgError):
             engine.set_tuning(warps_per_block=bad)
+
+
+@pytest.mark.parametrize("algo", ["plain", "learned"])
+def test_small_path_and_fallback(engine, algo):
+    """Products of at most small_rows rows take the small-product path (one
+    counting launch, a one-CTA scan, one numeric launch); a row of more than
+    2048 products sends the call to the binned pipeline; both match the
+    oracle bit for bit, in both index widths of C."""
+    engine.set_tuning(small_rows=0)
+    for name, A, B in PAIRS:
+        if name not in ("er4096", "stencil12", "wide_cols", "heavy_row", "empty", "zero_rows"):
+            continue
+        for bits in (0, 64):
+            C, rep = engine.multiply(A, B, algo=algo, use_tuning=True, out_index_bits=bits)
+            R = ref(name, A, B)
+            assert_parity(C.to_host(), R)
+            assert rep["nnz_c"] == R.nnz and rep["device_flags"] == 0
+            assert rep["products"] == int(gen.row_products(A, B).sum())
+            # heavy_row's first row has about 12,000 products; a product with no rows has nothing to do
+            assert rep["small_path"] == (0 if name in ("heavy_row", "zero_rows") else 1), (name, rep)
+            if rep["small_path"]:
+                assert rep["rows_predicted"] == 0
+    A = gen.erdos_renyi(4096, 4096, 8.0, 0)
+    engine.set_tuning(small_rows=4095)
+    C, rep = engine.multiply(A, A, algo=algo, use_tuning=True)
+    assert rep["small_path"] == 0
+    assert_parity(C.to_host(), ref("er4096", A, A))
+    engine.set_tuning(small_rows=-1)
+    C, rep = engine.multiply(A, A, algo=algo, use_tuning=True)
+    assert rep["small_path"] == 0
+    engine.set_tuning(small_rows=0)
+    for bad in (-2, 65537):
+        with pytest.raises(SpgError):
+            engine.set_tuning(small_rows=bad)
 
 
 @pytest.mark.parametrize("name,A,B", PAIRS[:9], ids=[p[0] for p in PAIRS[:9]])

@@ -294,6 +294,29 @@ spg_status spg_csr_transpose(const spg_csr* src, spg_csr* dst);
 spg_status spg_mtx_read(const char* path, spg_csr* out);
 
 /*
+ * COO -> CSR on the GPU.  n entries (0-based row_idx / col_idx, val) in any
+ * order, in host (location = SPG_HOST) or device (SPG_DEVICE) memory,
+ * become a device CSR of the context (int64 row_ptr, sorted columns) whose
+ * duplicate (i, j) pairs are summed in FP32 in the order given, the first
+ * value plus the second plus ... (as spg_mtx_read sums duplicates).
+ * Entries outside rows x cols fail with SPG_ERR_INVALID_ARG.  Replaces the
+ * reference's upload + cusparseXcoo2csr (cuSparse/src/main.cpp:408-442),
+ * which needs row-sorted input and keeps duplicates.  Free with
+ * spg_csr_free.
+ */
+spg_status spg_coo_to_csr(spg_ctx* ctx, int64_t rows, int64_t cols, int64_t n, const int32_t* row_idx,
+                          const int32_t* col_idx, const float* val, int32_t location, spg_csr* out);
+
+/*
+ * spg_mtx_read's parse (all host threads) followed by spg_coo_to_csr: the
+ * file's entries go to the GPU as COO and the CSR is built there, with the
+ * same result as spg_mtx_read uploaded (bit for bit).  Replaces the
+ * reference's reader + host-to-device copy + cusparseXcoo2csr
+ * (cuSparse/src/util.cpp:9-44, cuSparse/src/main.cpp:408-442).
+ */
+spg_status spg_mtx_read_device(spg_ctx* ctx, const char* path, spg_csr* out);
+
+/*
  * Writes `%%MatrixMarket matrix coordinate real general`, `rows cols nnz`,
  * then 1-based `i j v` lines in row-major order with sorted columns.
  * drop_zeros = 1 skips entries whose value is exactly 0, as the ray-tracing

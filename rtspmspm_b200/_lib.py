@@ -129,6 +129,9 @@ SIGNATURES = [
     ("spg_csr_download", ctypes.c_int32, [_vp, _P(SpgCsr), _vp, _vp, _vp]),
     ("spg_csr_extract_rows", ctypes.c_int32, [_vp, _P(SpgCsr), _vp, ctypes.c_int64, _P(SpgCsr)]),
     ("spg_mtx_read", ctypes.c_int32, [ctypes.c_char_p, _P(SpgCsr)]),
+    ("spg_mtx_read_device", ctypes.c_int32, [_vp, ctypes.c_char_p, _P(SpgCsr)]),
+    ("spg_coo_to_csr", ctypes.c_int32, [_vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, _vp, _vp, _vp,
+                                        ctypes.c_int32, _P(SpgCsr)]),
     ("spg_mtx_write", ctypes.c_int32, [_vp, ctypes.c_char_p, _P(SpgCsr), ctypes.c_int32]),
     ("spg_mlp_load", ctypes.c_int32, [_vp, ctypes.c_char_p]),
     ("spg_mlp_save", ctypes.c_int32, [_vp, ctypes.c_char_p]),

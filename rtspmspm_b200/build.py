@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
                      "-Xcompiler", "-Wall", "--expt-relaxed-constexpr", "-I" + INCLUDE]
 LIB_SOURCES = ["kernels.cu", "mlp.cu", "api.cu", "mlp_api.cu", "batched.cu",
-               "cusparse_ref.cu", "mtx_io.cpp", "tune.cpp", "noalloc.cu", "heavy.cu", "check.cu"]
+               "cusparse_ref.cu", "mtx_io.cpp", "tune.cpp", "noalloc.cu", "heavy.cu", "check.cu", "coo.cu"]
 
 
 def nvcc() -> str:

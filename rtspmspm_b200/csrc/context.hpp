@@ -87,6 +87,11 @@ class DevBuf {
 
 inline LaunchCtx launch_ctx(const spg_ctx* ctx) { return LaunchCtx{ctx->stream, ctx->sms}; }
 
+// Enqueues a copy of `bytes` (a multiple of 4) device bytes into the mapped
+// staging words at host_dst (inside ctx->h_stage); valid after the next
+// stream synchronisation.
+spg_status stage_read(spg_ctx* ctx, void* host_dst, const void* dev_src, size_t bytes);
+
 // Device view of an spg_csr already on the device with int64 row pointers.
 struct DevMat {
   DCsr view{};

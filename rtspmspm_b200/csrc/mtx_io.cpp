@@ -153,13 +153,17 @@ void run_workers(int n, F&& f) {
 
 }  // namespace
 
-// Parses the body in newline-aligned slices on all host threads, then builds
-// CSR: a counting sort by row keeps file order inside a row, and row blocks
-// (balanced by entries) are sorted by column and their duplicates summed in
-// file order in parallel.
-extern "C" spg_status spg_mtx_read(const char* path, spg_csr* out) {
-  if (!path || !out) return SPG_ERR_INVALID_ARG;
-  std::memset(out, 0, sizeof *out);
+// The parsed entries of a Matrix Market file: the header's shape and the
+// slices holding its first nnz entries (slices [0, last]), m of them after
+// the symmetric expansion.
+struct Parsed {
+  int64_t rows = 0, cols = 0, m = 0;
+  int last = -1;
+  std::vector<Slice> sl;
+};
+
+// Reads and parses `path` in newline-aligned slices on all host threads.
+spg_status parse_mtx(const char* path, Parsed& P) {
   std::vector<char> buf;
   if (!read_file(path, buf)) return SPG_ERR_IO;
   Cursor c{buf.data(), buf.data() + buf.size()};
@@ -202,7 +206,8 @@ extern "C" spg_status spg_mtx_read(const char* path, spg_csr* out) {
     while (q < c.end && q[-1] != '\n') ++q;
     cut[(size_t)t] = q;
   }
-  std::vector<Slice> sl((size_t)ns);
+  std::vector<Slice>& sl = P.sl;
+  sl.assign((size_t)ns, Slice());
   run_workers(ns, [&](int t) {
     parse_slice(cut[(size_t)t], cut[(size_t)t + 1], pattern, symmetric, skew, rows, cols, sl[(size_t)t]);
   });
@@ -228,6 +233,26 @@ extern "C" spg_status spg_mtx_read(const char* path, spg_csr* out) {
     m += (int64_t)sl[(size_t)t].ri.size();
   }
   if (seen < nnz) return SPG_ERR_FORMAT;
+  P.rows = rows;
+  P.cols = cols;
+  P.m = m;
+  P.last = last;
+  return SPG_OK;
+}
+
+// Parses the body in newline-aligned slices on all host threads, then builds
+// CSR: a counting sort by row keeps file order inside a row, and row blocks
+// (balanced by entries) are sorted by column and their duplicates summed in
+// file order in parallel.
+extern "C" spg_status spg_mtx_read(const char* path, spg_csr* out) {
+  if (!path || !out) return SPG_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof *out);
+  Parsed P;
+  const spg_status st = parse_mtx(path, P);
+  if (st != SPG_OK) return st;
+  const int64_t rows = P.rows, cols = P.cols, m = P.m;
+  const int last = P.last;
+  std::vector<Slice>& sl = P.sl;
   // ---- counting sort by row (stable: file order inside a row) ----
   std::vector<int64_t> rp((size_t)rows + 1, 0);
   for (int t = 0; t <= last; ++t)
@@ -319,6 +344,31 @@ extern "C" spg_status spg_mtx_read(const char* path, spg_csr* out) {
   out->val = hval;
   out->owner = 2;
   return SPG_OK;
+}
+
+// Parses on all host threads as spg_mtx_read does, then gathers the
+// slices' entries (file order, symmetric mirrors after their entry) into one
+// COO and builds the CSR on the GPU (spg_coo_to_csr): no host sort.
+extern "C" spg_status spg_mtx_read_device(spg_ctx* ctx, const char* path, spg_csr* out) {
+  if (!ctx || !path || !out) return SPG_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof *out);
+  Parsed P;
+  const spg_status st = parse_mtx(path, P);
+  if (st != SPG_OK) return st;
+  std::vector<int64_t> at((size_t)P.last + 2, 0);
+  for (int t = 0; t <= P.last; ++t) at[(size_t)t + 1] = at[(size_t)t] + (int64_t)P.sl[(size_t)t].ri.size();
+  std::vector<int32_t> ri((size_t)P.m), ci((size_t)P.m);
+  std::vector<float> vv((size_t)P.m);
+  if (P.last >= 0) run_workers(P.last + 1, [&](int t) {
+    const Slice& z = P.sl[(size_t)t];
+    const size_t o = (size_t)at[(size_t)t], k = z.ri.size();
+    if (!k) return;
+    std::memcpy(ri.data() + o, z.ri.data(), k * 4);
+    std::memcpy(ci.data() + o, z.ci.data(), k * 4);
+    std::memcpy(vv.data() + o, z.vv.data(), k * 4);
+  });
+  P.sl.clear();
+  return spg_coo_to_csr(ctx, P.rows, P.cols, P.m, ri.data(), ci.data(), vv.data(), SPG_HOST, out);
 }
 
 extern "C" spg_status spg_csr_transpose(const spg_csr* src, spg_csr* dst) {

@@ -410,6 +410,30 @@ class Engine:
                                     ctypes.byref(t)))
         return t.as_dict()
 
+    def coo_to_csr(self, rows: int, cols: int, row_idx, col_idx, val) -> Result:
+        """Device CSR from 0-based COO arrays in any order (numpy: uploaded,
+        or torch CUDA tensors: used in place), built on the GPU; duplicates
+        are summed in the order given."""
+        def ptr(x):
+            return x.data_ptr() if hasattr(x, "data_ptr") else x.ctypes.data
+
+        r = np.ascontiguousarray(row_idx, np.int32) if not hasattr(row_idx, "data_ptr") else row_idx
+        c = np.ascontiguousarray(col_idx, np.int32) if not hasattr(col_idx, "data_ptr") else col_idx
+        v = np.ascontiguousarray(val, np.float32) if not hasattr(val, "data_ptr") else val
+        loc = _lib.SPG_DEVICE if hasattr(row_idx, "data_ptr") and row_idx.is_cuda else _lib.SPG_HOST
+        n = len(r)
+        out = _lib.SpgCsr()
+        self._check(self.L.spg_coo_to_csr(self.ctx, int(rows), int(cols), int(n), ptr(r) if n else None,
+                                          ptr(c) if n else None, ptr(v) if n else None, loc, ctypes.byref(out)))
+        return Result(self, out)
+
+    def read_mtx_device(self, path: str) -> Result:
+        """Matrix Market file -> device CSR: parsed on the host threads, the
+        CSR built on the GPU from the file's COO."""
+        out = _lib.SpgCsr()
+        self._check(self.L.spg_mtx_read_device(self.ctx, os.fsencode(path), ctypes.byref(out)))
+        return Result(self, out)
+
     def write_mtx(self, path: str, C, drop_zeros: bool = False) -> None:
         s = C.s if isinstance(C, Result) else self._as_struct(C, self.device)[0]
         self._check(self.L.spg_mtx_write(self.ctx, path.encode(), ctypes.byref(s), int(drop_zeros)))

@@ -135,7 +135,9 @@ bool same_matrix(const spg_csr* a, const spg_csr* b) {
                     a->val == b->val);
 }
 
-spg_status prepare_matrix(spg_ctx* ctx, const spg_csr* m, DevMat& out, bool validate) {
+// defer_entries (host inputs): the column/value buffers are allocated but not
+// filled; the caller uploads them (spg_multiply_into_host's row chunks).
+spg_status prepare_matrix(spg_ctx* ctx, const spg_csr* m, DevMat& out, bool validate, bool defer_entries) {
   if (!m) return fail(ctx, SPG_ERR_INVALID_ARG, "null matrix");
   if (m->rows < 0 || m->cols < 0 || m->nnz < 0) return fail(ctx, SPG_ERR_INVALID_ARG, "negative dimension");
   if (m->cols > INT32_MAX) return fail(ctx, SPG_ERR_UNSUPPORTED, "more than 2^31-1 columns");
@@ -154,7 +156,7 @@ spg_status prepare_matrix(spg_ctx* ctx, const spg_csr* m, DevMat& out, bool vali
     SPG_TRY(out.upload[2].alloc(ctx, (size_t)m->nnz * 4));
     if (m->rows >= 0)
       SPG_CUDA(ctx, cudaMemcpyAsync(out.upload[0].get(), m->row_ptr, rp_bytes, cudaMemcpyHostToDevice, ctx->stream));
-    if (m->nnz > 0) {
+    if (m->nnz > 0 && !defer_entries) {
       SPG_CUDA(ctx, cudaMemcpyAsync(out.upload[1].get(), m->col_idx, (size_t)m->nnz * 4, cudaMemcpyHostToDevice,
                                     ctx->stream));
       SPG_CUDA(ctx, cudaMemcpyAsync(out.upload[2].get(), m->val, (size_t)m->nnz * 4, cudaMemcpyHostToDevice,
@@ -367,6 +369,8 @@ struct Pipeline {
     }
     const int64_t nheavy = bin_size(kBinHeavy);
     if (nheavy > 0) {
+      // the blocked index reads every row of B
+      if (B.complete) SPG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, B.complete, 0));
       size_t free_b = 0, total_b = 0;
       cudaMemGetInfo(&free_b, &total_b);
       // the list of non-empty (row, tile) units for the tile kernel, when it
@@ -883,6 +887,10 @@ spg_status spg_destroy(spg_ctx* ctx) {
   cudaFree(ctx->d_flags);
   cudaFree(ctx->d_counter);
   cudaFreeHost(ctx->h_stage);
+  if (ctx->upload_stream) {
+    cudaStreamSynchronize(ctx->upload_stream);
+    cudaStreamDestroy(ctx->upload_stream);
+  }
   if (ctx->copy_stream) {
     cudaStreamSynchronize(ctx->copy_stream);
     cudaStreamDestroy(ctx->copy_stream);
@@ -982,12 +990,58 @@ spg_status spg_multiply_into_host(spg_ctx* ctx, const spg_csr* A, const spg_csr*
   }
   const int launches0 = ctx->launches;
   DevMat dA, dB;
-  SPG_TRY(prepare_matrix(ctx, A, dA, !o.skip_validation));
   const bool same = same_matrix(A, B);
+  // A = B given once from host memory, validation off: the entries go up in
+  // the compute blocks' row chunks on an upload stream, so block b waits only
+  // for the chunks holding its own rows and the rows of B its columns reach,
+  // and the upload runs beside the downloads of earlier blocks (the host
+  // link carries both directions at once)
+  const bool chunked = same && A->location == SPG_HOST && o.skip_validation && A->nnz > 0 && blocks > 1 &&
+                       A->rows > 1;
+  SPG_TRY(prepare_matrix(ctx, A, dA, !o.skip_validation, chunked));
   if (!same) SPG_TRY(prepare_matrix(ctx, B, dB, !o.skip_validation));
   const DevMat& rB = same ? dA : dB;
   if (!o.skip_validation) SPG_TRY(check_flags(ctx, report));
   if (!ctx->copy_stream) SPG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  std::vector<cudaEvent_t> up_evs;  // one per row chunk, on the upload stream
+  struct UpEvents {
+    spg_ctx* ctx;
+    std::vector<cudaEvent_t>& evs;
+    ~UpEvents() {
+      if (!evs.empty()) cudaStreamSynchronize(ctx->upload_stream);
+      for (cudaEvent_t e : evs) cudaEventDestroy(e);
+    }
+  } up_guard{ctx, up_evs};
+  auto a_rp = [&](int64_t i) -> int64_t {
+    return A->index_bits == 64 ? static_cast<const int64_t*>(A->row_ptr)[i]
+                               : (int64_t) static_cast<const int32_t*>(A->row_ptr)[i];
+  };
+  const int64_t nb_rows = std::min<int64_t>(blocks, std::max<int64_t>(A->rows, 1));
+  if (chunked) {
+    if (!ctx->upload_stream) SPG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->upload_stream, cudaStreamNonBlocking));
+    // the device buffers come from the pool on ctx->stream
+    cudaEvent_t alloc_ev = nullptr;
+    SPG_CUDA(ctx, cudaEventCreateWithFlags(&alloc_ev, cudaEventDisableTiming));
+    up_evs.push_back(alloc_ev);
+    SPG_CUDA(ctx, cudaEventRecord(alloc_ev, ctx->stream));
+    SPG_CUDA(ctx, cudaStreamWaitEvent(ctx->upload_stream, alloc_ev, 0));
+    int32_t* dcol = dA.upload[1].as<int32_t>();
+    float* dval = dA.upload[2].as<float>();
+    for (int64_t b = 0; b < nb_rows; ++b) {
+      const int64_t e0 = a_rp(A->rows * b / nb_rows), e1 = a_rp(A->rows * (b + 1) / nb_rows);
+      if (e1 > e0) {
+        SPG_CUDA(ctx, cudaMemcpyAsync(dcol + e0, A->col_idx + e0, (size_t)(e1 - e0) * 4, cudaMemcpyHostToDevice,
+                                      ctx->upload_stream));
+        SPG_CUDA(ctx, cudaMemcpyAsync(dval + e0, A->val + e0, (size_t)(e1 - e0) * 4, cudaMemcpyHostToDevice,
+                                      ctx->upload_stream));
+      }
+      cudaEvent_t ev = nullptr;
+      SPG_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      up_evs.push_back(ev);
+      SPG_CUDA(ctx, cudaEventRecord(ev, ctx->upload_stream));
+    }
+    dA.complete = up_evs.back();
+  }
   const LaunchCtx lc = launch_ctx(ctx);
   const int64_t rows = A->rows;
   const int w = C->index_bits / 8;
@@ -1023,6 +1077,19 @@ spg_status spg_multiply_into_host(spg_ctx* ctx, const spg_csr* A, const spg_csr*
     Ab.view.rp = dA.view.rp + r0;
     Ab.view.rp32 = dA.view.rp32 ? dA.view.rp32 + r0 : nullptr;
     Ab.nnz = dA.nnz;
+    if (chunked) {
+      // rows of A keep ascending columns: a row's largest column is its last entry
+      int64_t last = r1 - 1;
+      for (int64_t r = r0; r < r1; ++r) {
+        const int64_t e = a_rp(r + 1);
+        if (e > a_rp(r)) last = std::max<int64_t>(last, A->col_idx[e - 1]);
+      }
+      last = std::min<int64_t>(last, rows - 1);
+      int64_t chunk = b;
+      while (chunk + 1 < nb && rows * (chunk + 1) / nb <= last) ++chunk;
+      st = cuda_status(ctx, cudaStreamWaitEvent(ctx->stream, up_evs[(size_t)chunk + 1], 0), "cudaStreamWaitEvent");
+      if (st != SPG_OK) break;
+    }
     spg_csr cb{};
     spg_report rb{};
     st = multiply_device(ctx, Ab, rB, &cb, o, report ? &rb : nullptr);

@@ -20,6 +20,7 @@ struct spg_ctx {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream = nullptr;  // device-to-host copies overlapped with compute (created on first use)
+  cudaStream_t upload_stream = nullptr;  // host-to-device copies of input row chunks (created on first use)
   cudaMemPool_t pool = nullptr;
   std::string last_error;
   std::string gpu_name;
@@ -99,12 +100,15 @@ struct DevMat {
   DevBuf rp64;      // widened row pointers when the input had int32 ones
   DevBuf rp32;      // narrowed row pointers when the input had int64 ones and nnz < 2^31
   DevBuf upload[3]; // copies of host inputs
+  // set while the entries are still being uploaded in row chunks: kernels
+  // that read every row (the heavy-row blocked index) wait for it
+  cudaEvent_t complete = nullptr;
 };
 
 // Prepares `m` for the kernels: uploads host data and widens int32 row
 // pointers.  `validate` runs the structure check kernel (flags raised on the
 // context's device flag word).
-spg_status prepare_matrix(spg_ctx* ctx, const spg_csr* m, DevMat& out, bool validate);
+spg_status prepare_matrix(spg_ctx* ctx, const spg_csr* m, DevMat& out, bool validate, bool defer_entries = false);
 
 // A and B describe the same matrix (same storage): prepare it once.
 bool same_matrix(const spg_csr* a, const spg_csr* b);

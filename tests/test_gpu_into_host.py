@@ -72,3 +72,30 @@ def test_into_host_empty_rows_and_more_blocks_than_rows(engine):
     rp, col, val = host_buffers(A.rows, max(R.nnz, 1), 64, pinned=False)
     nnz, _ = engine.multiply_into_host(A, A, rp, col, val, blocks=64, algo="plain")
     assert_parity(as_csr(A.rows, A.cols, rp, col, val, nnz), R)
+
+
+@pytest.mark.parametrize("algo", ["plain", "learned"])
+def test_into_host_chunked_upload(engine, algo):
+    """A = B from host memory with validation off goes up in row chunks
+    beside the compute: a banded matrix (each block waits for the next chunk
+    or two), a product with heavy rows whose blocked index reads every row of
+    B (it waits for the whole upload), and a random matrix (every block
+    reaches the last chunk) all match the oracle."""
+    cases = [(gen.stencil27(16, seed=4), {}), (gen.erdos_renyi(3000, 3000, 6.0, 13), {}),
+             (heavy_row(), {"warp_table_max": 64, "block_table_max": 1024, "block_min_nnz": -1, "small_rows": -1})]
+    for A, tune in cases:
+        saved = engine.get_tuning()
+        if tune:
+            engine.set_tuning(**tune)
+        try:
+            R = oracle.spgemm(A, A)
+            for pinned in (True, False):
+                rp, col, val = host_buffers(A.rows, R.nnz, 64, pinned=pinned)
+                nnz, rep = engine.multiply_into_host(A, A, rp, col, val, blocks=7, algo=algo, skip_validation=True,
+                                                     use_tuning=bool(tune))
+                assert nnz == R.nnz
+                assert_parity(as_csr(A.rows, A.cols, rp, col, val, nnz), R)
+            if tune:
+                assert rep["rows_heavy"] > 0
+        finally:
+            engine.set_tuning(**saved)

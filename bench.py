@@ -463,7 +463,7 @@ def main():
                     help="other configurations: one JSON line of per-method timings (not the headline)")
     ap.add_argument("--rmat-scale", type=int, default=20, help="scale of --workload rmat20 (smaller for profiling)")
     ap.add_argument("--batch-count", type=int, default=512, help="products of --workload batch512")
-    ap.add_argument("--e2e-blocks", type=int, default=16,
+    ap.add_argument("--e2e-blocks", type=int, default=8,
                     help="row blocks of the end-to-end call (device-to-host copy overlapped with the product)")
     args = ap.parse_args()
     if args.workload != "stencil96":

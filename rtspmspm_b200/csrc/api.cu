@@ -1016,7 +1016,9 @@ spg_status spg_multiply_into_host(spg_ctx* ctx, const spg_csr* A, const spg_csr*
     return A->index_bits == 64 ? static_cast<const int64_t*>(A->row_ptr)[i]
                                : (int64_t) static_cast<const int32_t*>(A->row_ptr)[i];
   };
-  const int64_t nb_rows = std::min<int64_t>(blocks, std::max<int64_t>(A->rows, 1));
+  // upload chunks: finer than the compute blocks, so that a block waits for
+  // little more than the rows it reaches
+  const int64_t nchunks = std::min<int64_t>(std::max<int64_t>(blocks, 64), std::max<int64_t>(A->rows, 1));
   if (chunked) {
     if (!ctx->upload_stream) SPG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->upload_stream, cudaStreamNonBlocking));
     // the device buffers come from the pool on ctx->stream
@@ -1027,8 +1029,8 @@ spg_status spg_multiply_into_host(spg_ctx* ctx, const spg_csr* A, const spg_csr*
     SPG_CUDA(ctx, cudaStreamWaitEvent(ctx->upload_stream, alloc_ev, 0));
     int32_t* dcol = dA.upload[1].as<int32_t>();
     float* dval = dA.upload[2].as<float>();
-    for (int64_t b = 0; b < nb_rows; ++b) {
-      const int64_t e0 = a_rp(A->rows * b / nb_rows), e1 = a_rp(A->rows * (b + 1) / nb_rows);
+    for (int64_t c = 0; c < nchunks; ++c) {
+      const int64_t e0 = a_rp(A->rows * c / nchunks), e1 = a_rp(A->rows * (c + 1) / nchunks);
       if (e1 > e0) {
         SPG_CUDA(ctx, cudaMemcpyAsync(dcol + e0, A->col_idx + e0, (size_t)(e1 - e0) * 4, cudaMemcpyHostToDevice,
                                       ctx->upload_stream));
@@ -1085,8 +1087,10 @@ spg_status spg_multiply_into_host(spg_ctx* ctx, const spg_csr* A, const spg_csr*
         if (e > a_rp(r)) last = std::max<int64_t>(last, A->col_idx[e - 1]);
       }
       last = std::min<int64_t>(last, rows - 1);
-      int64_t chunk = b;
-      while (chunk + 1 < nb && rows * (chunk + 1) / nb <= last) ++chunk;
+      // the chunk holding row `last` (chunks hold rows [rows*c/nchunks, rows*(c+1)/nchunks))
+      int64_t chunk = std::min<int64_t>(nchunks - 1, last * nchunks / rows);
+      while (chunk > 0 && rows * chunk / nchunks > last) --chunk;
+      while (chunk + 1 < nchunks && rows * (chunk + 1) / nchunks <= last) ++chunk;
       st = cuda_status(ctx, cudaStreamWaitEvent(ctx->stream, up_evs[(size_t)chunk + 1], 0), "cudaStreamWaitEvent");
       if (st != SPG_OK) break;
     }

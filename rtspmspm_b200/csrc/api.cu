@@ -1057,6 +1057,14 @@ spg_status spg_multiply_into_host(spg_ctx* ctx, const spg_csr* A, const spg_csr*
     return SPG_OK;
   }
   const int64_t nb = std::min<int64_t>(blocks, rows);
+  // block boundaries: the first block a quarter of the others (the first
+  // download starts sooner), the rest of the rows split evenly
+  const int64_t first = nb >= 2 ? std::max<int64_t>(1, rows / (4 * nb)) : rows;
+  auto block_start = [&](int64_t b) -> int64_t {
+    if (b <= 0) return 0;
+    if (b >= nb) return rows;
+    return first + (rows - first) * (b - 1) / (nb - 1);
+  };
   DevBuf rp_dev;  // C's row pointers in C's width, staged for the copies
   SPG_TRY(rp_dev.alloc(ctx, (size_t)(rows + 1) * w));
   std::vector<cudaEvent_t> evs;
@@ -1072,7 +1080,7 @@ spg_status spg_multiply_into_host(spg_ctx* ctx, const spg_csr* A, const spg_csr*
   bool overflow = false;
   spg_status st = SPG_OK;
   for (int64_t b = 0; b < nb && st == SPG_OK; ++b) {
-    const int64_t r0 = rows * b / nb, r1 = rows * (b + 1) / nb;
+    const int64_t r0 = block_start(b), r1 = block_start(b + 1);
     DevMat Ab;  // view of A's rows [r0, r1): row pointers index the full column/value arrays
     Ab.view = dA.view;
     Ab.view.rows = r1 - r0;

@@ -1057,14 +1057,9 @@ spg_status spg_multiply_into_host(spg_ctx* ctx, const spg_csr* A, const spg_csr*
     return SPG_OK;
   }
   const int64_t nb = std::min<int64_t>(blocks, rows);
-  // block boundaries: the first block a quarter of the others (the first
-  // download starts sooner), the rest of the rows split evenly
-  const int64_t first = nb >= 2 ? std::max<int64_t>(1, rows / (4 * nb)) : rows;
-  auto block_start = [&](int64_t b) -> int64_t {
-    if (b <= 0) return 0;
-    if (b >= nb) return rows;
-    return first + (rows - first) * (b - 1) / (nb - 1);
-  };
+  // even row blocks (a first block of a quarter the size, to start the
+  // first download sooner, measured 18.9 -> 19.3 ms on the stencil-96 call)
+  auto block_start = [&](int64_t b) -> int64_t { return rows * b / nb; };
   DevBuf rp_dev;  // C's row pointers in C's width, staged for the copies
   SPG_TRY(rp_dev.alloc(ctx, (size_t)(rows + 1) * w));
   std::vector<cudaEvent_t> evs;

@@ -161,17 +161,19 @@ __device__ __forceinline__ void acc_segment(const DCsr& B, Off bs, int len, floa
 
 // The chunk's n segments when each is one k-serial step (kPackBelow <= len
 // <= 32): step idx's B loads are issued before step idx - 1's table work, so
-// their latency overlaps it (stencil 96^3 plain numeric 3.90 -> 3.47 ms).
+// their latency overlaps it (stencil 96^3 plain numeric 3.90 -> 3.47 ms);
+// a step's length comes from the shuffle that fetched its loads (three
+// shuffles a step instead of four: learned numeric 3.34 -> 3.33 ms).
 template <int LOGT, bool LEARNED, typename Off>
 __device__ __forceinline__ void acc_single_steps(const DCsr& B, Off bs, int len, float a, int n, int32_t* keys,
                                                  float* vals, int epoch, bool& bad, int* flags) {
   const int lane = lane_id();
   int32_t jn = -1;
   float bn = 0.f;
+  int nl = __shfl_sync(kFull, len, 0);  // the next step's length, carried over
   {
     const Off sbs = __shfl_sync(kFull, bs, 0);
-    const int sl = __shfl_sync(kFull, len, 0);
-    if (lane < sl) {
+    if (lane < nl) {
       jn = B.col[sbs + lane];
       bn = B.val[sbs + lane];
     }
@@ -180,10 +182,10 @@ __device__ __forceinline__ void acc_single_steps(const DCsr& B, Off bs, int len,
     const int32_t j = jn;
     const float bv = bn;
     const float sa = __shfl_sync(kFull, a, idx);
-    const int sl = __shfl_sync(kFull, len, idx);
+    const int sl = nl;
     if (idx + 1 < n) {
       const Off nbs = __shfl_sync(kFull, bs, idx + 1);
-      const int nl = __shfl_sync(kFull, len, idx + 1);
+      nl = __shfl_sync(kFull, len, idx + 1);
       if (lane < nl) {
         jn = B.col[nbs + lane];
         bn = B.val[nbs + lane];

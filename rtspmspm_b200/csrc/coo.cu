@@ -24,6 +24,7 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;                       // per lane
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 entries per CTA
 constexpr int kDigits = 256;
+constexpr int kScatterSmem = kSortTile * (8 + 4);  // the tile's keys and values in digit order
 
 __global__ void k_coo_keys(const int32_t* ri, const int32_t* ci, int64_t n, int64_t rows, int64_t cols, uint64_t* key,
                            int* flags) {
@@ -55,18 +56,28 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint64_t* key
 
 // Stable scatter of one tile: warp w owns entries [w * 512, (w + 1) * 512)
 // of the tile, taken 32 consecutive at a time, so an entry's rank among the
-// tile's entries of its digit follows (warp, step, lane) = input order.
-// off: exclusive scan of hist (digit-major), the first output position of
-// each (digit, tile).
+// tile's entries of its digit follows (warp, step, lane) = input order.  The
+// tile is first ordered by digit in shared memory (entry at tile position
+// lp = the digit's first position in the tile + the counts of earlier warps
+// + the entry's rank), then written out by consecutive threads, so each
+// digit's run of the tile goes to consecutive global positions (coalesced
+// stores; scattering straight from registers ran at 1.1 TB/s).  off:
+// exclusive scan of hist (digit-major), the first output position of each
+// (digit, tile).  Dynamic shared memory: kSortTile keys and values.
 __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const uint64_t* kin, const float* vin, int64_t n,
                                                                 int shift, int64_t ntiles, const int64_t* off,
                                                                 uint64_t* kout, float* vout) {
-  __shared__ int64_t base[kSortWarps][kDigits];
+  __shared__ int base[kSortWarps][kDigits];
+  __shared__ int first[kDigits];  // the digit's first position in the tile's digit order
+  extern __shared__ uint64_t sm_sort[];
+  uint64_t* sk = sm_sort;
+  float* sv = reinterpret_cast<float*>(sm_sort + kSortTile);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   for (int d = lane; d < kDigits; d += 32) base[w][d] = 0;
   __syncwarp();
-  const int64_t w0 = blockIdx.x * (int64_t)kSortTile + (int64_t)w * (kSortItems * 32);
+  const int64_t t0 = blockIdx.x * (int64_t)kSortTile;
+  const int64_t w0 = t0 + (int64_t)w * (kSortItems * 32);
   uint64_t k[kSortItems];
   float v[kSortItems];
 #pragma unroll
@@ -85,33 +96,54 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const uint64_t* 
     __syncwarp();
   }
   __syncthreads();
-  // first position of each (warp, digit): the tile's offset plus the
-  // counts of the warps before it
+  // per digit: its total in the tile and, per warp, the start of the warp's entries
   {
     const int d = threadIdx.x;
-    int64_t run = off[(int64_t)d * ntiles + blockIdx.x];
+    int run = 0;
 #pragma unroll
     for (int x = 0; x < kSortWarps; ++x) {
-      const int64_t c = base[x][d];
+      const int c = base[x][d];
       base[x][d] = run;
       run += c;
     }
+    // exclusive scan of the digit totals across the CTA (digit d = thread d)
+    const int incl = warp_incl_scan(run);
+    __shared__ int wtot[kSortWarps];
+    if (lane == 31) wtot[w] = incl;
+    __syncthreads();
+    int pre = 0;
+#pragma unroll
+    for (int x = 0; x < kSortWarps; ++x) pre += x < w ? wtot[x] : 0;
+    first[d] = pre + incl - run;
   }
+  __syncthreads();
+  for (int d = threadIdx.x; d < kDigits; d += kSortThreads)
+    for (int x = 0; x < kSortWarps; ++x) base[x][d] += first[d];
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
     const bool act = w0 + j * 32 + lane < n;
     const int d = act ? (int)((k[j] >> shift) & 0xffu) : kDigits + lane;
     const unsigned grp = __match_any_sync(kFull, d);
-    int64_t pos = 0;
-    if (act) pos = base[w][d] + __popc(grp & lt);
+    int lp = 0;
+    if (act) lp = base[w][d] + __popc(grp & lt);
     __syncwarp();
     if (act) {
-      kout[pos] = k[j];
-      vout[pos] = v[j];
+      sk[lp] = k[j];
+      sv[lp] = v[j];
       if ((grp & lt) == 0u) base[w][d] += __popc(grp);
     }
     __syncwarp();
+  }
+  __syncthreads();
+  // the tile in digit order, written by consecutive threads
+  const int cnt = (int)min((int64_t)kSortTile, n - t0);
+  for (int q = threadIdx.x; q < cnt; q += kSortThreads) {
+    const uint64_t key = sk[q];
+    const int d = (int)((key >> shift) & 0xffu);
+    const int64_t pos = off[(int64_t)d * ntiles + blockIdx.x] + (q - first[d]);
+    kout[pos] = key;
+    vout[pos] = sv[q];
   }
 }
 
@@ -184,10 +216,11 @@ spg_status coo_to_csr_device(spg_ctx* ctx, int64_t rows, int64_t cols, int64_t n
   for (int s = 0; s < cbits; s += 8) shifts.push_back(s);
   for (int s = 0; s < rbits; s += 8) shifts.push_back(32 + s);
   if (n > 1) {
+    SPG_CUDA(ctx, cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, kScatterSmem));
     for (int shift : shifts) {
       k_radix_hist<<<(unsigned)ntiles, kSortThreads, 0, lc.stream>>>(kin, n, shift, ntiles, hist.as<int64_t>());
       launch_excl_scan(hist.as<int64_t>(), kDigits * ntiles, hist.as<int64_t>(), tmp.as<int64_t>(), lc);
-      k_radix_scatter<<<(unsigned)ntiles, kSortThreads, 0, lc.stream>>>(kin, vin, n, shift, ntiles,
+      k_radix_scatter<<<(unsigned)ntiles, kSortThreads, kScatterSmem, lc.stream>>>(kin, vin, n, shift, ntiles,
                                                                         hist.as<int64_t>(), kout, vout);
       std::swap(kin, kout);
       std::swap(vin, vout);

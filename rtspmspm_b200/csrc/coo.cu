@@ -21,7 +21,7 @@ namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 16;                       // per lane
+constexpr int kSortItems = 8;                        // per lane
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 entries per CTA
 constexpr int kDigits = 256;
 constexpr int kScatterSmem = kSortTile * (8 + 4);  // the tile's keys and values in digit order
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint64_t* key
   hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = cnt[threadIdx.x];
 }
 
-// Stable scatter of one tile: warp w owns entries [w * 512, (w + 1) * 512)
+// Stable scatter of one tile: warp w owns entries [w * 32 * kSortItems, (w + 1) * 32 * kSortItems)
 // of the tile, taken 32 consecutive at a time, so an entry's rank among the
 // tile's entries of its digit follows (warp, step, lane) = input order.  The
 // tile is first ordered by digit in shared memory (entry at tile position

@@ -386,7 +386,7 @@ def other_workload(args) -> int:
     rmat20 = C=A*A on R-MAT scale 20 (a=.57, b=c=.19, edge factor 16, seed 0);
     er4096 = C=A*A on the 4,096^2 Erdos-Renyi Poisson(8) matrix (seed 0);
     batch512 = 512 independent uneven products (seed 1) replayed from a CUDA
-    graph."""
+    graph; coo = COO -> CSR on the GPU of 2^26 random entries."""
     import torch
 
     from rtspmspm_b200 import DeviceCsr, Engine, gen
@@ -395,6 +395,28 @@ def other_workload(args) -> int:
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     out = {"workload": args.workload, "steps": args.steps, "warmup": args.warmup}
+    if args.workload == "coo":
+        # COO -> CSR on the GPU: 2^26 random entries over 2^22 x 2^22, device-resident
+        n, dim = 1 << 26, 1 << 22
+        g = torch.Generator(device="cuda").manual_seed(3)
+        r = torch.randint(0, dim, (n,), device="cuda", dtype=torch.int32, generator=g)
+        c = torch.randint(0, dim, (n,), device="cuda", dtype=torch.int32, generator=g)
+        v = torch.rand(n, device="cuda", generator=g)
+        holder = {}
+
+        def step():
+            C = eng.coo_to_csr(dim, dim, r, c, v)
+            holder["nnz"] = C.nnz
+            C.free()
+
+        for _ in range(args.warmup):
+            step()
+        ms = timed_median(step, args.steps, flush, stream)
+        out.update({"entries": n, "nnz_c": holder["nnz"], "ms": round(ms, 3),
+                    "entries_per_s": round(n / (ms * 1e-3), 1)})
+        print(json.dumps(out), flush=True)
+        eng.close()
+        return 0
     # --profile: one method only, default settings (short runs under ncu)
     only = [args.profile] if args.profile else ["plain", "learned"]
     if args.workload == "batch512":
@@ -459,7 +481,7 @@ def main():
                     help="skip the R-MAT-20 / ER-4096 / batch-512 timings that ride on the headline line")
     ap.add_argument("--profile", choices=["plain", "learned"], default=None,
                     help="only W warm-up + K steps of one method (short runs under ncu)")
-    ap.add_argument("--workload", choices=["stencil96", "rmat20", "er4096", "batch512"], default="stencil96",
+    ap.add_argument("--workload", choices=["stencil96", "rmat20", "er4096", "batch512", "coo"], default="stencil96",
                     help="other configurations: one JSON line of per-method timings (not the headline)")
     ap.add_argument("--rmat-scale", type=int, default=20, help="scale of --workload rmat20 (smaller for profiling)")
     ap.add_argument("--batch-count", type=int, default=512, help="products of --workload batch512")

@@ -407,10 +407,10 @@ typedef struct spg_tuning {
                                   output keeps half of them or more, and that fit the warp's
                                   table memory, are expanded, radix sorted on their columns and
                                   folded instead of hashed; -1: off */
-    int32_t small_rows;        /* products whose A has at most this many rows (0: default 8192),
-                                  every row of at most 2048 products, take the small-product
-                                  path in both methods (three launches, one host round trip);
-                                  -1: off */
+    int32_t small_rows;        /* products whose A has at most this many rows (0: default 8192;
+                                  at most 65536), every row of at most 2048 products, take the
+                                  small-product path in both methods (three launches, one host
+                                  round trip); -1: off */
 } spg_tuning;
 
 spg_status spg_get_tuning(spg_ctx* ctx, spg_tuning* out);
